@@ -1,0 +1,385 @@
+"""Benchmark of the SpMV hot path on B200 (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--format csr_naive] [--impl ours|reference]
+
+Workload: the 4M x 4M configuration of the reference's artificial generator (gamma row
+lengths, skew 100, seed 7; nnz 80,469,735), generated natively, values mapped to U[-1, 1),
+x ~ U[-1, 1).  A step is one SpMV y = A x over the whole matrix.
+
+Metric: SpMV GB/s over the algorithmic bytes of one SpMV,
+    B = nnz * (8 + 4) + (m + 1) * 4 + n * 8 + m * 8
+(the reference's csr_mem_footprint, spmv_kernel.h:23, plus x read once and y written once),
+and GFLOP/s = 2 nnz / t (bench_spmv.cpp:358).  `value` is measured on device-resident
+inputs with CUDA events around exactly K steps (after W warm-up steps); the inputs (1.05 GB)
+exceed the 126 MB L2, so no flush is needed between steps.  `e2e` is the same metric
+through the public API with host buffers: x copied host->device and y device->host inside
+every timed step.  Every format of the reference is converted and timed (`per_format`);
+the headline `value` is --format.
+
+--impl reference times the reference's own CPU implementation of the same format, compiled
+from its sources (oracle/_ref), on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+CONFIG2 = (4000000, 4000000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7)
+WORKLOAD = "config2: artificial 4Mx4M, avg 20, std 15, gamma, random, bw 0.05, skew 100, neigh 2.0, cross 0.3, seed 7"
+FORMATS = ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s", "div_rf"]
+FORMAT_PARAMS = {
+    "sell_c_s": dict(sellcs_c=32, sellcs_sigma=512),
+}
+FALLBACK_HBM = 6650.0
+
+
+def load_package():
+    if "spmv_dare_b200" in sys.modules:
+        return sys.modules["spmv_dare_b200"]
+    pkg = os.path.join(ROOT, "spmv-dare_b200")
+    spec = importlib.util.spec_from_file_location("spmv_dare_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["spmv_dare_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def algorithmic_bytes(m, n, nnz, vsize=8, xsize=8):
+    return nnz * (vsize + 4) + (m + 1) * 4 + n * xsize + m * xsize
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def ncu_traffic(fmt):
+    """dram bytes per launch of the format's kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"spmv_{fmt}_config2.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join("/tmp", f"spmv_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.send_signal(signal.SIGTERM)
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def generate(sb):
+    g = sb.generate_artificial(*CONFIG2)
+    v = 2.0 * g.values - 1.0
+    x = np.random.default_rng(12345).uniform(-1.0, 1.0, g.m)
+    return g.row_ptr, g.col_ind, v, x
+
+
+def time_device(mf, xd, yd, steps, warmup, torch):
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        mf.spmv(xd, yd)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for k in range(steps):
+        mf.spmv(xd, yd)
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+    total = ev[0].elapsed_time(ev[steps])
+    return total, per
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    sb = load_package()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    rp, ci, v, x = generate(sb)
+    m, n, nnz = rp.size - 1, rp.size - 1, int(rp[-1])
+    B = algorithmic_bytes(m, n, nnz)
+    flops = 2.0 * nnz
+    peak, peak_kind = hbm_peak()
+
+    formats = [args.format] + [f for f in FORMATS if f != args.format] if args.all_formats else [args.format]
+    per_format = {}
+    head = None
+    for fmt in formats:
+        try:
+            mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format=fmt, **FORMAT_PARAMS.get(fmt, {}))
+        except sb.SpmvError as e:
+            per_format[fmt] = {"error": str(e)}
+            continue
+        xd = torch.from_numpy(x).to(dev)
+        yd = torch.empty(m, dtype=torch.float64, device=dev)
+        sampler = ClockSampler(local) if fmt == args.format else None
+        barrier(world)
+        if sampler:
+            sampler.start()
+        total_ms, per = time_device(mf, xd, yd, args.steps, args.warmup, torch)
+        clocks = sampler.stop() if sampler else None
+        barrier(world)
+        total_ms = max_over_ranks(world, total_ms)
+        ms = total_ms / args.steps
+        med = statistics.median(per)
+        rec = {"ms_per_step": ms, "ms_median": med, "gbs": B * 1e-9 / (ms * 1e-3),
+               "gflops": flops * 1e-9 / (ms * 1e-3), "hbm_frac": B * 1e-9 / (med * 1e-3) / peak,
+               "convert_ms": mf.convert_ms, "mem_footprint": mf.mem_footprint, "stored_elems": mf.stored_elems,
+               "kernels_per_spmv": mf.kernels_per_run}
+        per_format[fmt] = rec
+        if fmt == args.format:
+            head = dict(rec, clocks=clocks, mf=mf, xd=xd, yd=yd, per=per)
+        else:
+            del mf
+        torch.cuda.empty_cache()
+
+    if head is None:
+        raise SystemExit(f"format {args.format} failed: {per_format.get(args.format)}")
+
+    # e2e: public API with pinned host buffers; x H2D and y D2H inside every step
+    mf = head["mf"]
+    xh = torch.from_numpy(x).pin_memory().numpy()
+    yh = torch.empty(m, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(args.warmup):
+        mf.spmv(xh, yh)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mf.spmv(xh, yh)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = max_over_ranks(world, e2e_s)
+
+    value = world * B * 1e-9 / (head["ms_per_step"] * 1e-3)
+    achieved = B * 1e-9 / (statistics.median(head["per"]) * 1e-3)
+    traffic = ncu_traffic(args.format)
+    out = {
+        "metric": "SpMV GB/s (algorithmic bytes / time; % of HBM peak in roofline)",
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(head["ms_per_step"], 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (the reference's artificial generator restated natively, config 2; values 2v-1, x U[-1,1))",
+        "config": {"workload": WORKLOAD, "format": args.format, "m": m, "n": n, "nnz": nnz,
+                   "bytes_per_spmv": B, "gflops": round(head["gflops"], 2),
+                   "l2": "no flush: inputs (1.05 GB/SpMV) exceed the 126 MB L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "format_params": FORMAT_PARAMS.get(args.format, {})},
+        "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s", "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_s * 1e3, 4)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s"},
+        "gpu_launches": args.steps * mf.kernels_per_run,
+        "clocks": head["clocks"],
+        "per_format": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in r.items()}
+                       for k, r in per_format.items()},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.format, rp, ci, v, x, B, sample_s=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline(fmt, rp, ci, v, x, B, sample_s=10.0):
+    """The reference's own CPU implementation (compiled from its sources into oracle/_ref),
+    all host cores, timed like bench_spmv.cpp:316-358 (median iteration)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    cores = len(os.sched_getaffinity(0))
+    name = fmt if fmt in ("csr_naive", "csr_vec", "sell", "sell_sorted", "div_rf") else "csr_naive"
+    if not O.ref_available(name):
+        return {"value": None, "unit": "GB/s", "cores": cores, "kind": "reference",
+                "sample": f"unavailable: oracle/_ref/libref_{name}.so not built"}
+    R = O.RefFormat(name, rp, ci, v, threads=cores)
+    y = np.ones(R.m + 64)
+    R.spmv(x, y)
+    times = []
+    t_end = time.perf_counter() + sample_s
+    while time.perf_counter() < t_end or len(times) < 5:
+        t0 = time.perf_counter()
+        R.spmv(x, y)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": round(B * 1e-9 / med, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+            "format": name, "ms_median": round(med * 1e3, 3),
+            "sample": f"config 2 full matrix, {len(times)} SpMV iterations over ~{sample_s:.0f} s, median"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    name = args.format if args.format in ("csr_naive", "csr_vec", "sell", "sell_sorted", "div_rf") else "csr_naive"
+    if not O.ref_available(name) or not O.ref_available("gen"):
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build oracle/_ref/libref_{name}.so missing"}))
+        return
+    cores = len(os.sched_getaffinity(0))
+    rp, ci, v, st = O.ref_generate(*CONFIG2[:4], CONFIG2[4], CONFIG2[5], *CONFIG2[6:10], CONFIG2[10], threads=cores)
+    v = 2.0 * v - 1.0
+    m = n = rp.size - 1
+    nnz = int(rp[-1])
+    x = np.random.default_rng(12345).uniform(-1.0, 1.0, n)
+    B = algorithmic_bytes(m, n, nnz)
+    R = O.RefFormat(name, rp, ci, v, threads=cores)
+    y = np.ones(m + 64)
+    for _ in range(args.warmup):
+        R.spmv(x, y)
+    per = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        R.spmv(x, y)
+        per.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(per) / len(per)
+    val = B * 1e-9 / (ms * 1e-3)
+    out = {
+        "metric": "SpMV GB/s (algorithmic bytes / time; % of HBM peak in roofline)",
+        "value": round(val, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (the reference's own generator, config 2; values 2v-1, x U[-1,1))",
+        "config": {"workload": WORKLOAD, "format": name, "m": m, "n": n, "nnz": nnz, "bytes_per_spmv": B},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                         "sample": f"config 2 full matrix, {args.steps} timed SpMV steps after {args.warmup} warm-up"},
+        "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--format", default="csr_naive", choices=FORMATS)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--all-formats", dest="all_formats", action="store_true", default=True)
+    ap.add_argument("--only-format", dest="all_formats", action="store_false")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

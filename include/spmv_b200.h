@@ -1,0 +1,206 @@
+/*
+ * spmv_b200.h -- C ABI of the B200-native SpMV engine (libspmv_b200.so).
+ *
+ * This is the drop-in boundary for the reference's format plugin API:
+ *
+ *   struct Matrix_Format * csr_to_format(INT_T * row_ptr, INT_T * col_ind,
+ *           ValueTypeReference * values, long m, long n, long nnz,
+ *           long symmetric, long symmetry_expanded);           src/spmv_kernels/spmv_kernel.h:28
+ *   virtual void Matrix_Format::spmv(ValueType * x, ValueType * y);   spmv_kernel.h:17
+ *   double Matrix_Format::mem_footprint / csr_mem_footprint;         spmv_kernel.h:13-14,23
+ *   char * Matrix_Format::format_name;                                spmv_kernel.h:10
+ *   int statistics_print_labels(char * buf, long buf_n);              spmv_kernel.h:29
+ *   int Matrix_Format::statistics_print_data(char * buf, long buf_n); spmv_kernel.h:19
+ *
+ * spmv_create() replaces csr_to_format() (the conversion runs on the GPU); spmv_run()
+ * replaces Matrix_Format::spmv() for host buffers; spmv_run_device() is the
+ * device-resident variant.  All entry points are plain C: pointers, sizes and status
+ * codes, no CUDA or torch types.  Streams are passed as `void *` (a cudaStream_t).
+ *
+ * Errors: every entry point returns (or writes through `status`) one of SPMV_OK /
+ * SPMV_ERR_*; spmv_last_error() gives the message of the calling thread's last error.
+ * The reference instead prints and exits (error(), e.g. csr.cpp:131-132); the C++
+ * plugin shim maps a non-zero status back to that behaviour.
+ */
+#ifndef SPMV_B200_H
+#define SPMV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define SPMV_OK                0
+#define SPMV_ERR_ARG           1   /* invalid argument or parameter combination             */
+#define SPMV_ERR_CSR           2   /* malformed CSR: row_ptr not monotone / col out of range */
+#define SPMV_ERR_CUDA          3   /* CUDA runtime error                                     */
+#define SPMV_ERR_NOMEM         4   /* device allocation failed                               */
+#define SPMV_ERR_UNSUPPORTED   5   /* e.g. symmetric input that is not expanded (csr.cpp:131) */
+#define SPMV_ERR_TIMEOUT       6   /* a bounded device wait gave up                          */
+#define SPMV_ERR_BOUNDS        7   /* a device-side bounds check fired                       */
+#define SPMV_ERR_NO_DEVICE     8   /* no CUDA device                                         */
+#define SPMV_ERR_OVERFLOW      9   /* a converted array exceeds the 32-bit index range       */
+
+/* ---------------------------------------------------------------- formats */
+/* One id per reference format executable (src/Makefile_in:47-74, config.sh:183-196). */
+#define SPMV_FMT_CSR_NAIVE     0   /* src/spmv_kernels/csr.cpp                    */
+#define SPMV_FMT_CSR_VEC       1   /* src/spmv_kernels/csr_vec.cpp                */
+#define SPMV_FMT_SELL          2   /* src/spmv_kernels/sell.cpp                   */
+#define SPMV_FMT_SELL_SORTED   3   /* src/spmv_kernels/sell_sorted.cpp            */
+#define SPMV_FMT_SELL_C_S      4   /* src/spmv_kernels/sell_c_s.cpp + sell-C-s/   */
+#define SPMV_FMT_DIV_RF        5   /* src/spmv_kernels/DIV/div.cpp, DIV_TYPE_RF   */
+#define SPMV_NUM_FORMATS       6
+
+/* Value storage of a handle. */
+#define SPMV_VALUES_F64        0   /* FP64 values and arithmetic: the drop-in                 */
+#define SPMV_VALUES_F32        1   /* FP32 values, FP32 products, TwoSum-compensated row sums */
+
+/*
+ * Conversion parameters.  spmv_format_desc_init() fills the reference's defaults; the
+ * layout-defining ones are those of the reference's x86 AVX2 build:
+ *   num_threads      T   the OpenMP thread count the reference converts with; it defines
+ *                        the thread ranges that sell / sell_sorted / div_rf layouts depend on
+ *                        (sell.cpp:161, sell_sorted.cpp:164-180, div.cpp:263).   default 8
+ *   vec_len          V/L csr_vec lanes, SELL slice height, DIV-RF lanes (VEC_LEN;
+ *                        vectorization_x86_avx256_f64.h:22).                     default 4
+ *   sellcs_c         C   SELL-C-sigma slice height, a power of two <= 256.       default 32
+ *   sellcs_sigma     s   SELL-C-sigma sorting window, a multiple of C.           default 512
+ *                        (the reference hard-codes C=256, s=16384 at sell_c_s.cpp:58-60)
+ *   div_packet_vals      CSRCV_NUM_PACKET_VALS (config.sh:150).                  default 16384
+ *   div_tolerance        DIV_VC_TOLERANCE, lossy value rounding (config.sh:123). default 0
+ *   exact                1: every row is summed in the reference format's own order
+ *                        (bit-identical y); 0: rows longer than one staged block are
+ *                        reduced in parallel (tolerance parity).                   default 1
+ *   values               SPMV_VALUES_F64 or SPMV_VALUES_F32.                       default F64
+ *   block_nnz, block_rows, stages, ctas_per_sm: kernel tuning knobs, 0 = default.
+ */
+typedef struct spmv_format_desc {
+	int32_t format;
+	int32_t num_threads;
+	int32_t vec_len;
+	int32_t sellcs_c;
+	int32_t sellcs_sigma;
+	int32_t div_packet_vals;
+	double  div_tolerance;
+	int32_t exact;
+	int32_t values;
+	int32_t block_nnz;
+	int32_t block_rows;
+	int32_t stages;
+	int32_t ctas_per_sm;
+	int32_t reserved[8];
+} spmv_format_desc;
+
+typedef struct spmv_handle spmv_handle;
+
+/* Per-handle information (Matrix_Format's public fields plus GPU facts). */
+typedef struct spmv_info {
+	int64_t m, n, nnz;
+	double  mem_footprint;       /* bytes of the converted format (format-specific, as the reference) */
+	double  csr_mem_footprint;   /* nnz*(sizeof(value)+4) + (m+1)*4  (spmv_kernel.h:23)          */
+	int64_t stored_elems;        /* stored (padded) entries for sliced formats; nnz otherwise    */
+	int64_t device_bytes;        /* device memory held by the handle                             */
+	double  convert_ms;          /* GPU conversion time (host->device copy included)             */
+	int32_t kernels_per_run;     /* kernel launches one spmv_run_device() makes                  */
+	int32_t format;
+	char    format_name[64];     /* the reference's format_name, e.g. "Naive_CSR_CPU" -> "Naive_CSR_GPU" */
+} spmv_info;
+
+/* Fill *desc with the defaults above for `format`. */
+void spmv_format_desc_init(spmv_format_desc * desc, int32_t format);
+
+/*
+ * csr_to_format: validate and convert a HOST CSR matrix (borrowed: it is copied, as every
+ * reference format deep-copies, csr.cpp:55-66) into the requested GPU format on the
+ * current CUDA device.  symmetric && !symmetry_expanded is rejected with
+ * SPMV_ERR_UNSUPPORTED, as every reference format rejects it (csr.cpp:131).
+ * Returns NULL on error with *status set.
+ */
+spmv_handle * spmv_create(const int32_t * row_ptr, const int32_t * col_ind, const double * values,
+		int64_t m, int64_t n, int64_t nnz, int64_t symmetric, int64_t symmetry_expanded,
+		const spmv_format_desc * desc, int * status);
+
+/* As spmv_create, with the CSR arrays already in device memory (read-only, borrowed). */
+spmv_handle * spmv_create_device(const int32_t * d_row_ptr, const int32_t * d_col_ind, const double * d_values,
+		int64_t m, int64_t n, int64_t nnz, const spmv_format_desc * desc, void * stream, int * status);
+
+/* Matrix_Format::spmv(x, y) with HOST buffers: x[n] -> device, y[m] <- device, synchronous.
+ * Rows without entries get 0 (the reference's y=1.0 probe, bench_spmv.cpp:561-564). */
+int spmv_run(spmv_handle * h, const double * x, double * y);
+
+/* Device-resident SpMV: d_x[n], d_y[m] in device memory, enqueued on `stream` (NULL =
+ * the handle's stream); returns after the launch.  Errors raised by device-side checks
+ * are reported by the next spmv_sync() / spmv_run(). */
+int spmv_run_device(spmv_handle * h, const double * d_x, double * d_y, void * stream);
+
+/* FP32 variant entry: float x / y (values stored FP32, handle created with values = F32). */
+int spmv_run_device_f32(spmv_handle * h, const float * d_x, float * d_y, void * stream);
+
+/* Waits for the handle's stream and returns the first device-side error, if any. */
+int spmv_sync(spmv_handle * h);
+
+int spmv_get_info(const spmv_handle * h, spmv_info * out);
+
+/*
+ * Copies one converted array to host memory, for array-for-array parity with the
+ * reference's csr_to_format.  If dst is NULL only *count (elements) is written.
+ * Array ids and element types:
+ */
+#define SPMV_ARR_ROW_PTR          0   /* int32[m+1]           CSR                                */
+#define SPMV_ARR_COL_IND          1   /* int32[nnz]           CSR                                */
+#define SPMV_ARR_VALUES           2   /* f64[nnz] / f32[nnz]  CSR                                */
+#define SPMV_ARR_SELL_PTR        10   /* int32[clusters+1]    sell, sell_sorted: row_cluster_ptr  */
+#define SPMV_ARR_SELL_JA         11   /* int32[nnz_ext]       ja                                 */
+#define SPMV_ARR_SELL_A          12   /* f64[nnz_ext]         a                                  */
+#define SPMV_ARR_SELL_PERM       13   /* int32[m]             sell_sorted: permutation           */
+#define SPMV_ARR_SELL_REV_PERM   14   /* int32[m]             sell_sorted: rev_permutation       */
+#define SPMV_ARR_THREAD_RANGES   15   /* int64[2T]            per-thread [start, end)            */
+#define SPMV_ARR_SELLCS_ORDER    20   /* int32[m]             row_order                          */
+#define SPMV_ARR_SELLCS_WIDTHS   21   /* int32[slices]        slice_widths                       */
+#define SPMV_ARR_SELLCS_PTR      22   /* int64[slices+1]      slice_pointers                     */
+#define SPMV_ARR_SELLCS_COLS     23   /* int32[size]          column_indices                     */
+#define SPMV_ARR_SELLCS_VALS     24   /* f64[size]            values                             */
+#define SPMV_ARR_DIV_DATA        30   /* uint8[bytes]         all threads' packet streams, in thread order */
+#define SPMV_ARR_DIV_PACKETS     31   /* int64[packets+1]     packet byte offsets                */
+#define SPMV_ARR_DIV_GROUPS      32   /* int64[...]           each thread's packet-group offsets (groups+1 each) */
+#define SPMV_ARR_DIV_THREAD_BYTES 33  /* int64[T]             bytes per thread                   */
+#define SPMV_ARR_DIV_THREAD_GROUPS 34 /* int64[T]             packet groups per thread           */
+int spmv_export(const spmv_handle * h, int32_t array_id, void * dst, int64_t * count);
+
+void spmv_destroy(spmv_handle * h);
+
+/* Message of the calling thread's last error ("" if none). */
+const char * spmv_last_error(void);
+
+/* Matrix_Format statistics hooks (spmv_kernel.h:18-19,29): CSV labels / values of the GPU
+ * run (launches, stored entries, bytes moved per SpMV).  Return the characters written. */
+int spmv_statistics_print_labels(char * buf, int64_t buf_n);
+int spmv_statistics_print_data(const spmv_handle * h, char * buf, int64_t buf_n);
+
+/* ---------------------------------------------------------------- artificial matrices */
+/*
+ * The reference's artificial matrix generator, restated natively on the host
+ * (artificial-matrix-generator/artificial_matrix_generation.c:163-579, argv order of
+ * src/bench.cpp:564-578).  Output is independent of the thread count.  Two calls:
+ * spmv_artgen_create() generates and returns an opaque result (NULL + *status on error);
+ * spmv_artgen_get() copies its arrays (row_ptr int32[rows+1], col int32[nnz],
+ * values f64[nnz], any may be NULL) and 37 structural statistics (may be NULL).
+ */
+typedef struct spmv_artgen spmv_artgen;
+spmv_artgen * spmv_artgen_create(int64_t rows, int64_t cols, double avg_nnz_per_row, double std_nnz_per_row,
+		const char * distribution, const char * placement, double bw, double skew,
+		double avg_num_neighbours, double cross_row_similarity, uint32_t seed, int num_threads, int * status);
+int64_t spmv_artgen_nnz(const spmv_artgen * g);
+int spmv_artgen_get(const spmv_artgen * g, int32_t * row_ptr, int32_t * col_ind, double * values, double * stats);
+void spmv_artgen_destroy(spmv_artgen * g);
+
+/* Library version string. */
+const char * spmv_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPMV_B200_H */

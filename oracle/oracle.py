@@ -215,6 +215,35 @@ def div_convert(rp, ci, v, n=None, T=8, L=4, packet_vals=16384, tolerance=0.0):
                 ranges=rg, T=T, L=L)
 
 
+def div_packet_offsets(data, L):
+    """Byte offsets of the packets of a DIV-RF stream (walking the headers,
+    div_kernels_rf.h:65-79 and :909-917); the last entry is the stream length."""
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    hsz = 28 + 4 * L
+    offs = [0]
+    pos = 0
+    while pos < data.size:
+        h = data[pos:pos + hsz]
+        u32 = lambda o: int.from_bytes(h[o:o + 4].tobytes(), "little")
+        nv, nu, nrf = u32(0), u32(4), u32(24)
+        cb = (int(h[20]) + int(h[21]) + 7) >> 3
+        lanes = sum(u32(28 + 4 * l) for l in range(L))
+        pos += hsz + 8 * nrf + cb * nv + nu + lanes
+        offs.append(pos)
+    if pos != data.size:
+        raise ValueError("DIV-RF stream does not end on a packet boundary")
+    return np.array(offs, np.int64)
+
+
+def div_zero_header_padding(data, L):
+    """The two padding bytes after col_bits in struct packet_header are never written by the
+    reference (their content is whatever the reused buffer held); zero them."""
+    data = np.array(data, dtype=np.uint8, copy=True)
+    for o in div_packet_offsets(data, L)[:-1]:
+        data[o + 22:o + 24] = 0
+    return data
+
+
 def div_spmv(arr, m, x, fused=False):
     x = _c(x, np.float64)
     y = np.ones(m, np.float64)

@@ -762,7 +762,7 @@ static long div_compress_packet(const int32_t * rp, const int32_t * ci, const do
 	long * lane_len = (long *) calloc(L, sizeof(long));
 	uint8_t ** lane_buf = (uint8_t **) malloc(L * sizeof(uint8_t *));
 	for (long l = 0; l < L; l++)
-		lane_buf[l] = (uint8_t *) malloc(8 * (nuniq / L + 2));
+		lane_buf[l] = (uint8_t *) malloc(8 * (nuniq / L + num_rfs + 1));   /* ceil per rf group */
 	uint64_t * prev = (uint64_t *) malloc(L * sizeof(uint64_t));
 	long ks = 0;
 	for (long g = 0; g < num_rfs; g++) {
@@ -948,7 +948,7 @@ void orc_div_free(void * hp)
  * running sum of its decoded differences (reset per group); the vector part visits blocks
  * of L unique values and, for each of the rf replicas, the L lanes in order; the
  * remaining values are visited one by one.  Calls emit(row, col, value) in that order. */
-typedef void (*div_emit_fn)(void * ctx, long row, long col, double val);
+typedef void (*div_emit_fn)(void * ctx, long row, long col, double val, int single_row);
 
 static long div_decode_packet(const uint8_t * buf, long L, div_emit_fn emit, void * ctx, long * nv_out)
 {
@@ -1000,7 +1000,7 @@ static long div_decode_packet(const uint8_t * buf, long L, div_emit_fn emit, voi
 						memcpy(&c, coords + k * cbytes, cbytes);
 						union { uint64_t u; double d; } vv;
 						vv.u = val[ln];
-						emit(ctx, row_min + (long) (c & rmask), col_min + (long) ((c >> row_bits) & cmask), vv.d);
+						emit(ctx, row_min + (long) (c & rmask), col_min + (long) ((c >> row_bits) & cmask), vv.d, row_bits == 0);
 					}
 			} else {
 				for (long j = 0; j < rf; j++) {
@@ -1009,7 +1009,7 @@ static long div_decode_packet(const uint8_t * buf, long L, div_emit_fn emit, voi
 					memcpy(&c, coords + k * cbytes, cbytes);
 					union { uint64_t u; double d; } vv;
 					vv.u = val[lane];
-					emit(ctx, row_min + (long) (c & rmask), col_min + (long) ((c >> row_bits) & cmask), vv.d);
+					emit(ctx, row_min + (long) (c & rmask), col_min + (long) ((c >> row_bits) & cmask), vv.d, row_bits == 0);
 				}
 			}
 		}
@@ -1024,10 +1024,14 @@ static long div_decode_packet(const uint8_t * buf, long L, div_emit_fn emit, voi
 
 struct spmv_ctx { const double * x; double * y; int fused; };
 
-static void emit_spmv(void * c, long row, long col, double val)
+/* The reference's x86 build fuses the multiply-add of packets that span several rows, but
+ * for single-row packets (row_bits == 0, the gather returns row 0 for every lane) the
+ * compiler turns the lane updates of y[row_min] into rounded products followed by
+ * rounded adds; both are reproduced here. */
+static void emit_spmv(void * c, long row, long col, double val, int single_row)
 {
 	struct spmv_ctx * s = (struct spmv_ctx *) c;
-	if (s->fused)
+	if (s->fused && !single_row)
 		s->y[row] = fma(val, s->x[col], s->y[row]);
 	else {
 		double p = val * s->x[col];
@@ -1055,8 +1059,9 @@ int orc_div_spmv(const uint8_t * data, long total, const int64_t * ranges, long 
 
 struct coo_ctx { int32_t * r; int32_t * c; double * v; long k; };
 
-static void emit_coo(void * cp, long row, long col, double val)
+static void emit_coo(void * cp, long row, long col, double val, int single_row)
 {
+	(void) single_row;
 	struct coo_ctx * s = (struct coo_ctx *) cp;
 	s->r[s->k] = (int32_t) row;
 	s->c[s->k] = (int32_t) col;

@@ -1,0 +1,308 @@
+"""spmv-dare_b200 -- B200-native SpMV engine behind the reference's format plugin API.
+
+Host-side mirror of the reference's plugin interface (src/spmv_kernels/spmv_kernel.h:8-29):
+
+    MF = csr_to_format(row_ptr, col_ind, values, m, n, nnz, symmetric, symmetry_expanded,
+                       format="csr_naive", ...)
+    MF.spmv(x, y)                 # Matrix_Format::spmv
+    MF.mem_footprint, MF.csr_mem_footprint, MF.format_name, MF.m, MF.n, MF.nnz
+    MF.statistics_start(); MF.statistics_print_data()
+    statistics_print_labels()
+
+Every call goes through the C ABI of libspmv_b200.so (include/spmv_b200.h).  The
+conversion and the SpMV run on the GPU; there is no CPU fallback: without the built
+library or without a CUDA device the calls raise.
+
+``spmv(x, y)`` accepts host numpy arrays (the reference's contract: x and y are host
+buffers, copied to and from the device inside the call) or CUDA torch tensors (the
+device-resident path, enqueued on torch's current stream).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_int, c_int64
+
+import numpy as np
+
+from . import _capi
+from ._capi import FORMATS, VALUES_F32, VALUES_F64
+
+__all__ = [
+    "SpmvError", "Matrix_Format", "csr_to_format", "statistics_print_labels", "generate_artificial",
+    "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version",
+]
+
+
+class SpmvError(RuntimeError):
+    """Raised for every non-zero status of the C ABI (the reference prints and exits)."""
+
+    def __init__(self, status, message):
+        super().__init__(f"[status {status}] {message}")
+        self.status = status
+
+
+def library():
+    return _capi.load()
+
+
+def version():
+    return library().spmv_version().decode()
+
+
+def _raise(status):
+    msg = library().spmv_last_error().decode(errors="replace")
+    raise SpmvError(status, msg or "error")
+
+
+def format_defaults(format="csr_naive"):
+    """The reference's defaults for `format` as a dict of descriptor fields."""
+    d = _capi.FormatDesc()
+    library().spmv_format_desc_init(byref(d), FORMATS[format])
+    return {name: getattr(d, name) for name, _ in _capi.FormatDesc._fields_ if name != "reserved"}
+
+
+def _desc(format, params):
+    if format not in FORMATS:
+        raise ValueError(f"unknown format {format!r}; one of {sorted(FORMATS)}")
+    d = _capi.FormatDesc()
+    library().spmv_format_desc_init(byref(d), FORMATS[format])
+    for k, v in params.items():
+        if v is None:
+            continue
+        if k == "values":
+            v = {"f64": VALUES_F64, "f32": VALUES_F32}.get(v, v)
+        if not hasattr(d, k) or k in ("format", "reserved"):
+            raise TypeError(f"unknown format parameter {k!r}")
+        setattr(d, k, v)
+    return d
+
+
+def _host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _is_cuda_tensor(a):
+    return getattr(a, "is_cuda", False) is True
+
+
+class Matrix_Format:
+    """A matrix converted to one GPU format (the reference's struct Matrix_Format)."""
+
+    def __init__(self, handle, format):
+        self._h = handle
+        self._format = format
+        info = _capi.Info()
+        st = library().spmv_get_info(self._h, byref(info))
+        if st:
+            _raise(st)
+        self.m = int(info.m)
+        self.n = int(info.n)
+        self.nnz = int(info.nnz)
+        self.mem_footprint = float(info.mem_footprint)
+        self.csr_mem_footprint = float(info.csr_mem_footprint)
+        self.format_name = info.format_name.decode()
+        self.stored_elems = int(info.stored_elems)
+        self.device_bytes = int(info.device_bytes)
+        self.convert_ms = float(info.convert_ms)
+        self.kernels_per_run = int(info.kernels_per_run)
+        self.num_loops = 0
+
+    @property
+    def format(self):
+        return self._format
+
+    @property
+    def handle(self):
+        return self._h
+
+    def spmv(self, x, y=None, stream=None):
+        """y = A x.  Host numpy buffers: synchronous copy-in / copy-out (Matrix_Format::spmv).
+        CUDA torch tensors: enqueued on `stream` (default: torch's current stream)."""
+        if self._h is None:
+            raise SpmvError(_capi.SPMV_ERR_ARG, "matrix already destroyed")
+        self.num_loops += 1
+        lib = library()
+        if _is_cuda_tensor(x):
+            import torch
+
+            if y is None:
+                y = torch.empty(self.m, dtype=x.dtype, device=x.device)
+            if not (x.is_contiguous() and y.is_contiguous()):
+                raise ValueError("x and y must be contiguous")
+            if x.numel() < self.n or y.numel() < self.m:
+                raise ValueError(f"x needs {self.n} and y {self.m} elements")
+            s = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
+            if x.dtype == torch.float32:
+                st = lib.spmv_run_device_f32(self._h, x.data_ptr(), y.data_ptr(), s)
+            else:
+                if x.dtype != torch.float64 or y.dtype != torch.float64:
+                    raise TypeError("x and y must both be float64 (or both float32 for the FP32 variant)")
+                st = lib.spmv_run_device(self._h, x.data_ptr(), y.data_ptr(), s)
+            if st:
+                _raise(st)
+            return y
+        xh = _host(x, np.float64)
+        if xh.size < self.n:
+            raise ValueError(f"x needs {self.n} elements")
+        if y is None:
+            y = np.empty(self.m, np.float64)
+        if not (isinstance(y, np.ndarray) and y.dtype == np.float64 and y.flags.c_contiguous and y.size >= self.m):
+            raise ValueError("y must be a contiguous float64 numpy array with at least m elements")
+        st = lib.spmv_run(self._h, xh.ctypes.data, y.ctypes.data)
+        if st:
+            _raise(st)
+        return y
+
+    def sync(self):
+        st = library().spmv_sync(self._h)
+        if st:
+            _raise(st)
+
+    def export(self, name):
+        """One converted array as numpy (for array-for-array parity with the reference)."""
+        aid, dt = _capi.ARRAYS[name]
+        if name == "values" and self._format == "csr_naive" and getattr(self, "_f32", False):
+            dt = "float32"
+        cnt = c_int64(0)
+        st = library().spmv_export(self._h, aid, None, byref(cnt))
+        if st:
+            _raise(st)
+        out = np.empty(max(cnt.value, 1), dtype=dt)
+        st = library().spmv_export(self._h, aid, out.ctypes.data, byref(cnt))
+        if st:
+            _raise(st)
+        return out[: cnt.value]
+
+    def statistics_start(self):
+        self.num_loops = 0
+
+    def statistics_print_data(self):
+        buf = ctypes.create_string_buffer(1024)
+        library().spmv_statistics_print_data(self._h, buf, len(buf))
+        return buf.value.decode()
+
+    def destroy(self):
+        if self._h is not None:
+            library().spmv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __repr__(self):
+        return f"<Matrix_Format {self.format_name} m={self.m} n={self.n} nnz={self.nnz}>"
+
+
+def csr_to_format(row_ptr, col_ind, values, m=None, n=None, nnz=None, symmetric=0, symmetry_expanded=1,
+                  format="csr_naive", **params):
+    """csr_to_format (spmv_kernel.h:28): convert a CSR matrix to `format` on the GPU.
+
+    Inputs may be host arrays (copied, as every reference format deep-copies) or CUDA torch
+    tensors (converted device-to-device).  `params` are spmv_format_desc fields
+    (num_threads, vec_len, sellcs_c, sellcs_sigma, div_packet_vals, div_tolerance, exact,
+    values, block_nnz, block_rows, stages, ctas_per_sm)."""
+    desc = _desc(format, params)
+    st = c_int(0)
+    lib = library()
+    if _is_cuda_tensor(row_ptr):
+        import torch
+
+        m = int(row_ptr.numel() - 1) if m is None else int(m)
+        nnz = int(col_ind.numel()) if nnz is None else int(nnz)
+        n = m if n is None else int(n)
+        if symmetric and not symmetry_expanded:
+            raise SpmvError(_capi.SPMV_ERR_UNSUPPORTED,
+                            "symmetric matrices have to be expanded to be supported by this format")
+        rp = row_ptr.contiguous()
+        ci = col_ind.contiguous()
+        vv = values.contiguous()
+        if rp.dtype != torch.int32 or ci.dtype != torch.int32 or vv.dtype != torch.float64:
+            raise TypeError("device CSR must be int32 row_ptr / col_ind and float64 values")
+        h = lib.spmv_create_device(rp.data_ptr(), ci.data_ptr(), vv.data_ptr(), m, n, nnz, byref(desc),
+                                   torch.cuda.current_stream(rp.device).cuda_stream, byref(st))
+    else:
+        rp = _host(row_ptr, np.int32)
+        ci = _host(col_ind, np.int32)
+        vv = _host(values, np.float64)
+        m = rp.size - 1 if m is None else int(m)
+        nnz = int(rp[m]) if nnz is None else int(nnz)
+        n = m if n is None else int(n)
+        h = lib.spmv_create(rp.ctypes.data, ci.ctypes.data if ci.size else None,
+                            vv.ctypes.data if vv.size else None, m, n, nnz, int(symmetric), int(symmetry_expanded),
+                            byref(desc), byref(st))
+    if not h:
+        _raise(st.value)
+    mf = Matrix_Format(h, format)
+    mf._f32 = desc.values == VALUES_F32
+    return mf
+
+
+def statistics_print_labels():
+    buf = ctypes.create_string_buffer(1024)
+    library().spmv_statistics_print_labels(buf, len(buf))
+    return buf.value.decode()
+
+
+STAT_NAMES = [
+    "avg_nnz_per_row", "std_nnz_per_row", "min_nnz_per_row", "max_nnz_per_row", "skew",
+    "avg_bw", "std_bw", "min_bw", "max_bw",
+    "avg_sc", "std_sc", "min_sc", "max_sc",
+    "avg_num_neighbours", "std_num_neighbours", "min_num_neighbours", "max_num_neighbours",
+    "cross_row_similarity", "std_cross_row_similarity", "min_cross_row_similarity", "max_cross_row_similarity",
+    "avg_clustering", "std_clustering", "min_clustering", "max_clustering",
+    "avg_ngroups", "std_ngroups", "min_ngroups", "max_ngroups",
+    "avg_dis", "std_dis", "min_dis", "max_dis",
+    "avg_ngroups_size", "std_ngroups_size", "min_ngroups_size", "max_ngroups_size",
+]
+
+
+class ArtificialMatrix:
+    """CSR arrays and structural statistics of one generated matrix."""
+
+    def __init__(self, row_ptr, col_ind, values, stats, params):
+        self.row_ptr = row_ptr
+        self.col_ind = col_ind
+        self.values = values
+        self.stats = stats
+        self.params = params
+
+    @property
+    def m(self):
+        return self.row_ptr.size - 1
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+
+def generate_artificial(rows, cols, avg_nnz_per_row, std_nnz_per_row, distribution, placement, avg_bw, skew,
+                        avg_num_neighbours, cross_row_similarity, seed, threads=0):
+    """The reference's artificial matrix generator (bench argv order, src/bench.cpp:564-578),
+    restated natively; thread-count independent.  Values are U[0,1) as in the reference."""
+    import os
+
+    lib = library()
+    st = c_int(0)
+    threads = threads or (os.cpu_count() or 1)
+    g = lib.spmv_artgen_create(int(rows), int(cols), float(avg_nnz_per_row), float(std_nnz_per_row),
+                               distribution.encode(), placement.encode(), float(avg_bw), float(skew),
+                               float(avg_num_neighbours), float(cross_row_similarity), int(seed) & 0xFFFFFFFF,
+                               int(threads), byref(st))
+    if not g:
+        _raise(st.value)
+    try:
+        nnz = lib.spmv_artgen_nnz(g)
+        rp = np.empty(rows + 1, np.int32)
+        ci = np.empty(max(nnz, 1), np.int32)
+        v = np.empty(max(nnz, 1), np.float64)
+        stats = np.empty(37, np.float64)
+        lib.spmv_artgen_get(g, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, stats.ctypes.data)
+    finally:
+        lib.spmv_artgen_destroy(g)
+    params = dict(rows=rows, cols=cols, avg_nnz_per_row=avg_nnz_per_row, std_nnz_per_row=std_nnz_per_row,
+                  distribution=distribution, placement=placement, avg_bw=avg_bw, skew=skew,
+                  avg_num_neighbours=avg_num_neighbours, cross_row_similarity=cross_row_similarity, seed=seed)
+    return ArtificialMatrix(rp, ci[:nnz], v[:nnz], dict(zip(STAT_NAMES, stats.tolist())), params)

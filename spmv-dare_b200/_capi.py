@@ -1,0 +1,106 @@
+"""ctypes declarations of the C ABI in include/spmv_b200.h (libspmv_b200.so)."""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char, c_char_p, c_double, c_int, c_int32, c_int64, c_uint32, c_void_p
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libspmv_b200.so")
+
+# status codes
+SPMV_OK = 0
+SPMV_ERR_ARG = 1
+SPMV_ERR_CSR = 2
+SPMV_ERR_CUDA = 3
+SPMV_ERR_NOMEM = 4
+SPMV_ERR_UNSUPPORTED = 5
+SPMV_ERR_TIMEOUT = 6
+SPMV_ERR_BOUNDS = 7
+SPMV_ERR_NO_DEVICE = 8
+SPMV_ERR_OVERFLOW = 9
+
+# formats (one per reference executable)
+FORMATS = {
+    "csr_naive": 0,
+    "csr_vec": 1,
+    "sell": 2,
+    "sell_sorted": 3,
+    "sell_c_s": 4,
+    "div_rf": 5,
+}
+
+VALUES_F64 = 0
+VALUES_F32 = 1
+
+# exportable arrays: name -> (id, numpy dtype)
+ARRAYS = {
+    "row_ptr": (0, "int32"), "col_ind": (1, "int32"), "values": (2, "float64"),
+    "row_cluster_ptr": (10, "int32"), "ja": (11, "int32"), "a": (12, "float64"),
+    "permutation": (13, "int32"), "rev_permutation": (14, "int32"), "ranges": (15, "int64"),
+    "row_order": (20, "int32"), "slice_widths": (21, "int32"), "slice_pointers": (22, "int64"),
+    "column_indices": (23, "int32"), "sellcs_values": (24, "float64"),
+    "div_data": (30, "uint8"), "div_packets": (31, "int64"), "div_groups": (32, "int64"),
+    "div_thread_bytes": (33, "int64"), "div_thread_groups": (34, "int64"),
+}
+
+
+class FormatDesc(ctypes.Structure):
+    _fields_ = [
+        ("format", c_int32), ("num_threads", c_int32), ("vec_len", c_int32), ("sellcs_c", c_int32),
+        ("sellcs_sigma", c_int32), ("div_packet_vals", c_int32), ("div_tolerance", c_double),
+        ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
+        ("stages", c_int32), ("ctas_per_sm", c_int32), ("reserved", c_int32 * 8),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("m", c_int64), ("n", c_int64), ("nnz", c_int64), ("mem_footprint", c_double),
+        ("csr_mem_footprint", c_double), ("stored_elems", c_int64), ("device_bytes", c_int64),
+        ("convert_ms", c_double), ("kernels_per_run", c_int32), ("format", c_int32),
+        ("format_name", c_char * 64),
+    ]
+
+
+# every exported entry point of include/spmv_b200.h: name -> (restype, argtypes)
+SIGNATURES = {
+    "spmv_format_desc_init": (None, [POINTER(FormatDesc), c_int32]),
+    "spmv_create": (c_void_p, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64, c_int64,
+                               POINTER(FormatDesc), POINTER(c_int)]),
+    "spmv_create_device": (c_void_p, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64,
+                                      POINTER(FormatDesc), c_void_p, POINTER(c_int)]),
+    "spmv_run": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "spmv_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_run_device_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_sync": (c_int, [c_void_p]),
+    "spmv_get_info": (c_int, [c_void_p, POINTER(Info)]),
+    "spmv_export": (c_int, [c_void_p, c_int32, c_void_p, POINTER(c_int64)]),
+    "spmv_destroy": (None, [c_void_p]),
+    "spmv_last_error": (c_char_p, []),
+    "spmv_statistics_print_labels": (c_int, [c_char_p, c_int64]),
+    "spmv_statistics_print_data": (c_int, [c_void_p, c_char_p, c_int64]),
+    "spmv_artgen_create": (c_void_p, [c_int64, c_int64, c_double, c_double, c_char_p, c_char_p, c_double, c_double,
+                                      c_double, c_double, c_uint32, c_int, POINTER(c_int)]),
+    "spmv_artgen_nnz": (c_int64, [c_void_p]),
+    "spmv_artgen_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_artgen_destroy": (None, [c_void_p]),
+    "spmv_version": (c_char_p, []),
+}
+
+_lib = None
+
+
+def load():
+    """Load libspmv_b200.so (raises if it has not been built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libspmv_b200.so is not built ({LIB_PATH}); run `python spmv-dare_b200/build.py`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib

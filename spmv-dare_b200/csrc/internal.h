@@ -1,0 +1,129 @@
+// Internal state of a converted matrix (the GPU counterpart of one Matrix_Format object).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace spmv {
+
+// A staged block: rows (or slices) [unit0, unit0 + units) whose stored entries
+// [elem0, elem0 + elems) are copied to shared memory in one bulk transfer.  units < 0
+// marks a long unit (one row / one slice larger than the staging capacity), processed
+// straight from global memory.
+struct StagedBlock {
+	int32_t unit0;
+	int32_t units;
+	int32_t elem0;
+	int32_t elems;
+};
+
+enum class Kind { CSR = 0, SLICED = 1 };
+enum class Arith { SEQ_SPLIT = 0, SEQ_FMA = 1, LANES_FMA = 2 };
+
+struct Handle {
+	spmv_format_desc desc{};
+	int64_t m = 0, n = 0, nnz = 0;
+	int device = 0;
+	int num_sms = 0;
+	cudaStream_t stream = nullptr;
+	int * d_err = nullptr;       // device error word
+
+	// CSR (csr_naive, csr_vec) -- also kept for sell/sell_sorted/sell_c_s conversions
+	int32_t * d_rp = nullptr;
+	int32_t * d_ci = nullptr;
+	double * d_v = nullptr;
+	float * d_vf = nullptr;      // FP32 variant values
+
+	// staged kernel
+	StagedBlock * d_blocks = nullptr;
+	int64_t num_blocks = 0;
+	int grid = 0;
+	int block_cap = 0;           // staging capacity in entries
+	int stages = 0;
+	size_t smem_bytes = 0;
+
+	// SELL / sell_sorted (slice height V)
+	int64_t nclusters = 0;
+	int64_t nnz_ext = 0;
+	int32_t * d_rcp = nullptr;   // row_cluster_ptr[nclusters+1]
+	int32_t * d_ja = nullptr;
+	double * d_a = nullptr;
+	int32_t * d_perm = nullptr;
+	int32_t * d_rev = nullptr;
+	int64_t * d_ranges = nullptr; // 2T thread ranges
+
+	// SELL-C-sigma
+	int64_t nslices = 0;
+	int64_t sellcs_size = 0;
+	int32_t * d_order = nullptr;
+	int32_t * d_widths = nullptr;
+	int64_t * d_sptr = nullptr;
+	int32_t * d_scols = nullptr;
+	double * d_svals = nullptr;
+
+	// DIV-RF
+	int64_t div_bytes = 0;
+	int64_t num_packets = 0;
+	uint8_t * d_div = nullptr;
+	int64_t * d_pkt = nullptr;          // packet byte offsets [num_packets+1]
+	int4 * d_pkt_meta = nullptr;        // per packet: {y row start, y row end, flags, 0}
+	int64_t * d_groups = nullptr;       // per-thread group offsets (concatenated)
+	int64_t num_group_entries = 0;
+	int64_t * d_thread_bytes = nullptr;
+	int64_t * d_thread_groups = nullptr;
+	int32_t * d_zero_rows = nullptr;    // rows not covered by any packet (zeroed each run)
+	int64_t num_zero_rows = 0;
+	double * d_split_part = nullptr;    // partial sums of rows split across packets
+	int32_t * d_split_rows = nullptr;
+	int64_t num_split = 0;
+
+	// host-buffer path staging
+	double * d_x = nullptr;
+	double * d_y = nullptr;
+
+	std::vector<void *> allocations;    // everything above, freed by destroy
+	double mem_footprint = 0;
+	double csr_mem_footprint = 0;
+	int64_t stored_elems = 0;
+	int64_t device_bytes = 0;
+	double convert_ms = 0;
+	int kernels_per_run = 0;
+	std::string name;
+
+	template <typename T>
+	int alloc(T ** p, int64_t count)
+	{
+		size_t bytes = (size_t) (count > 0 ? count : 1) * sizeof(T);
+		cudaError_t e = cudaMalloc((void **) p, bytes);
+		if (e != cudaSuccess) {
+			*p = nullptr;
+			set_error(SPMV_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+			return SPMV_ERR_NOMEM;
+		}
+		allocations.push_back((void *) *p);
+		device_bytes += (int64_t) bytes;
+		return SPMV_OK;
+	}
+};
+
+// ---- conversions (each fills the format's device arrays from d_rp/d_ci/d_v)
+int convert_csr(Handle & h);
+int convert_sell(Handle & h, bool sorted);
+int convert_sellcs(Handle & h);
+int convert_div(Handle & h);
+
+// ---- staged-block construction over a CSR row pointer or a slice pointer
+int build_csr_blocks(Handle & h, const int32_t * d_rowptr, int64_t rows);
+int build_slice_blocks(Handle & h, const int32_t * d_sliceptr, int64_t slices, int V);
+
+// ---- SpMV launches
+int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
+int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s);
+int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
+
+// Validates a device CSR: row_ptr[0] == 0, monotone, row_ptr[m] == nnz, 0 <= col < n.
+int validate_csr(Handle & h);
+
+}  // namespace spmv

@@ -1,0 +1,428 @@
+// SpMV kernels for B200 (sm_100a).
+//
+// staged_kernel  -- CSR (csr_naive, csr_vec) and narrow SELL slices (sell, sell_sorted with
+//                   V < 32).  Persistent CTAs walk a table of row blocks; each block's
+//                   stored entries are one contiguous range, brought into shared memory by
+//                   the bulk-copy engine (cp.async.bulk, mbarrier completion) while the CTA
+//                   computes the previous block.  Every output row is then summed by ONE
+//                   thread in the reference format's own operation order, so y is
+//                   bit-identical to the reference:
+//                     csr_naive  : sum = sum + a*x, product and sum rounded separately
+//                                  (subkernel_csr_scalar, src/spmv_kernels/csr.cpp:167-182,
+//                                  as the reference's x86 build evaluates it);
+//                     csr_vec    : L lanes of fused a*x+s, (s0+s2)+(s1+s3), split tail
+//                                  (subkernel_row_csr_vec, csr_vec.cpp:183-211);
+//                     sell(_sorted): one fused a*x+s per slice column, padding included
+//                                  (compute_sell, sell.cpp:240-280, sell_sorted.cpp:346-427).
+// sliced_kernel  -- slices of >= 32 rows (SELL-C-sigma; SELL with V >= 32): one thread per
+//                   row, a warp reads 32 consecutive column-major entries per step
+//                   (coalesced), fused multiply-add over the slice width as vfmacc does
+//                   (sellcs_mv_d, sell-C-s/sellcs_mv_kernels_epi.c:209-317).
+#include "internal.h"
+
+namespace spmv {
+
+namespace {
+
+constexpr int STAGED_THREADS = 256;
+
+struct StagedArgs {
+	const StagedBlock * blocks;
+	int64_t nblocks;
+	const int32_t * ptr;     // CSR: row_ptr; SLICED: row_cluster_ptr
+	const int32_t * cols;
+	const double * vals;
+	const int32_t * ymap;    // sell_sorted: rev_permutation
+	const double * x;
+	double * y;
+	int64_t m;
+	int V;                   // slice height (SLICED)
+	int cap_al;              // staged entries per stage buffer (capacity + alignment slack)
+	int stages;
+	int stage_bytes;
+	int exact;
+	int * err;
+};
+
+template <int L>
+__device__ __forceinline__ double lanes_reduce(const double * s)
+{
+	if (L == 1)
+		return s[0];
+	if (L == 2)
+		return s[0] + s[1];
+	if (L == 4)
+		return (s[0] + s[2]) + (s[1] + s[3]);
+	double tot = 0;
+	#pragma unroll
+	for (int h = 0; h < L; h += 4)
+		tot = tot + ((s[h] + s[h + 2]) + (s[h + 1] + s[h + 3]));
+	return tot;
+}
+
+// Sum of one CSR row whose entries are vals[js..je), cols[js..je) (shared or global).
+template <Arith A, int L>
+__device__ __forceinline__ double csr_row(const double * __restrict__ vals, const int32_t * __restrict__ cols, int64_t js,
+		int64_t je, const double * __restrict__ x)
+{
+	if (A == Arith::LANES_FMA) {
+		double s[L];
+		#pragma unroll
+		for (int l = 0; l < L; l++)
+			s[l] = 0.0;
+		int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
+		for (int64_t j = js; j < jv; j += L) {
+			#pragma unroll
+			for (int l = 0; l < L; l++)
+				s[l] = __fma_rn(vals[j + l], ldg(x + cols[j + l]), s[l]);
+		}
+		double sum = lanes_reduce<L>(s);
+		for (int64_t j = jv; j < je; j++)
+			sum = __dadd_rn(sum, __dmul_rn(vals[j], ldg(x + cols[j])));
+		return sum;
+	} else if (A == Arith::SEQ_FMA) {
+		double sum = 0.0;
+		#pragma unroll 4
+		for (int64_t j = js; j < je; j++)
+			sum = __fma_rn(vals[j], ldg(x + cols[j]), sum);
+		return sum;
+	} else {
+		double sum = 0.0;
+		#pragma unroll 4
+		for (int64_t j = js; j < je; j++)
+			sum = __dadd_rn(sum, __dmul_rn(vals[j], ldg(x + cols[j])));
+		return sum;
+	}
+}
+
+__device__ __forceinline__ void staged_issue(const StagedArgs & a, int64_t b, int s, uint8_t * smem, uint64_t * bars)
+{
+	StagedBlock d = a.blocks[b];
+	if (d.units < 0 || d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	uint32_t cnt = (uint32_t) (e1 - e0);
+	double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
+	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 12u);
+	bulk_g2s(sv, a.vals + e0, cnt * 8u, &bars[s]);
+	bulk_g2s(sc, a.cols + e0, cnt * 4u, &bars[s]);
+}
+
+// Deterministic CTA sum (fixed tree order).
+__device__ __forceinline__ double cta_sum(double v, double * red)
+{
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_down_sync(0xffffffffu, v, o);
+	if (lane == 0)
+		red[w] = v;
+	__syncthreads();
+	double t = 0;
+	if (threadIdx.x == 0) {
+		for (int i = 0; i < (int) (blockDim.x >> 5); i++)
+			t += red[i];
+	}
+	__syncthreads();
+	return t;
+}
+
+template <Kind K, Arith A, int L, bool YMAP>
+__global__ void __launch_bounds__(STAGED_THREADS) staged_kernel(StagedArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	__shared__ double red[STAGED_THREADS / 32];
+	uint64_t * bars = reinterpret_cast<uint64_t *>(smem + (size_t) a.stages * a.stage_bytes);
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < a.stages; s++)
+			mbar_init(&bars[s], 1);
+		mbar_fence_init();
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < a.stages; s++) {
+			int64_t b = (int64_t) blockIdx.x + (int64_t) s * gridDim.x;
+			if (b < a.nblocks)
+				staged_issue(a, b, s, smem, bars);
+		}
+	}
+
+	int it = 0;
+	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x, it++) {
+		const int s = it % a.stages;
+		const uint32_t parity = (uint32_t) ((it / a.stages) & 1);
+		const StagedBlock d = a.blocks[b];
+		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
+		if (__syncthreads_or(!ok)) {
+			if (threadIdx.x == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		if (d.units >= 0) {
+			const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+			const double * sv = reinterpret_cast<const double *>(smem + (size_t) s * a.stage_bytes);
+			const int32_t * sc = reinterpret_cast<const int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+			if (K == Kind::CSR) {
+				for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
+					const int64_t r = (int64_t) d.unit0 + u;
+					const int64_t js = (int64_t) a.ptr[r] - e0, je = (int64_t) a.ptr[r + 1] - e0;
+					a.y[r] = csr_row<A, L>(sv, sc, js, je, a.x);
+				}
+			} else {
+				const int V = a.V;
+				const int nrow = d.units * V;
+				for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
+					const int64_t sl = (int64_t) d.unit0 + u / V;
+					const int lane = u % V;
+					const int64_t row = sl * V + lane;
+					if (row >= a.m)
+						continue;
+					const int64_t ks = (int64_t) a.ptr[sl] - e0 + lane;
+					const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+					double acc = 0.0;
+					#pragma unroll 4
+					for (int k = 0; k < w; k++)
+						acc = __fma_rn(sv[ks + (int64_t) k * V], ldg(a.x + sc[ks + (int64_t) k * V]), acc);
+					a.y[YMAP ? a.ymap[row] : row] = acc;
+				}
+			}
+		} else {
+			// A unit larger than the staging capacity, straight from global memory.
+			if (K == Kind::CSR) {
+				const int64_t r = d.unit0;
+				const int64_t js = a.ptr[r], je = a.ptr[r + 1];
+				if (a.exact) {
+					if (threadIdx.x == 0)
+						a.y[r] = csr_row<A, L>(a.vals, a.cols, js, je, a.x);
+				} else {
+					double part = 0.0;
+					for (int64_t j = js + threadIdx.x; j < je; j += blockDim.x)
+						part = __fma_rn(a.vals[j], ldg(a.x + a.cols[j]), part);
+					double t = cta_sum(part, red);
+					if (threadIdx.x == 0)
+						a.y[r] = t;
+				}
+			} else {
+				const int V = a.V;
+				const int64_t sl = d.unit0;
+				const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+				for (int lane = threadIdx.x; lane < V; lane += blockDim.x) {
+					const int64_t row = sl * V + lane;
+					if (row >= a.m)
+						continue;
+					double acc = 0.0;
+					for (int k = 0; k < w; k++) {
+						const int64_t q = (int64_t) a.ptr[sl] + (int64_t) k * V + lane;
+						acc = __fma_rn(a.vals[q], ldg(a.x + a.cols[q]), acc);
+					}
+					a.y[YMAP ? a.ymap[row] : row] = acc;
+				}
+			}
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			int64_t nb = b + (int64_t) a.stages * gridDim.x;
+			if (nb < a.nblocks)
+				staged_issue(a, nb, s, smem, bars);
+		}
+	}
+}
+
+struct SlicedArgs {
+	const int64_t * sptr;    // slice pointers (SELL-C-sigma) or nullptr
+	const int32_t * rcp;     // row_cluster_ptr (SELL) or nullptr
+	const int32_t * widths;  // slice widths (SELL-C-sigma) or nullptr
+	const int32_t * cols;
+	const double * vals;
+	const int32_t * ymap;    // row_order / rev_permutation or nullptr
+	const double * x;
+	double * y;
+	int64_t m;
+	int64_t nslices;
+	int C;
+};
+
+template <bool PTR64, bool YMAP>
+__global__ void __launch_bounds__(256) sliced_kernel(SlicedArgs a)
+{
+	const int C = a.C;
+	const int spc = blockDim.x / C;
+	const int lane = threadIdx.x % C;
+	const int sl = threadIdx.x / C;
+	for (int64_t s = (int64_t) blockIdx.x * spc + sl; s < a.nslices; s += (int64_t) gridDim.x * spc) {
+		const int64_t row = s * C + lane;
+		if (row >= a.m)
+			continue;
+		int64_t p;
+		int w;
+		if (PTR64) {
+			p = a.sptr[s];
+			w = a.widths[s];
+		} else {
+			p = a.rcp[s];
+			w = (a.rcp[s + 1] - a.rcp[s]) / C;
+		}
+		p += lane;
+		const double * __restrict__ v = a.vals + p;
+		const int32_t * __restrict__ c = a.cols + p;
+		double acc = 0.0;
+		int k = 0;
+		for (; k + 4 <= w; k += 4) {
+			const int64_t o = (int64_t) k * C;
+			double v0 = v[o], v1 = v[o + C], v2 = v[o + 2 * C], v3 = v[o + 3 * C];
+			int32_t c0 = c[o], c1 = c[o + C], c2 = c[o + 2 * C], c3 = c[o + 3 * C];
+			double x0 = ldg(a.x + c0), x1 = ldg(a.x + c1), x2 = ldg(a.x + c2), x3 = ldg(a.x + c3);
+			acc = __fma_rn(v0, x0, acc);
+			acc = __fma_rn(v1, x1, acc);
+			acc = __fma_rn(v2, x2, acc);
+			acc = __fma_rn(v3, x3, acc);
+		}
+		for (; k < w; k++) {
+			const int64_t o = (int64_t) k * C;
+			acc = __fma_rn(v[o], ldg(a.x + c[o]), acc);
+		}
+		a.y[YMAP ? a.ymap[row] : row] = acc;
+	}
+}
+
+using StagedFn = void (*)(StagedArgs);
+
+// The staged kernel instance of a handle's format / lane count.
+StagedFn pick_staged(const Handle & h)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_CSR_NAIVE)
+		return staged_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+	if (fmt == SPMV_FMT_CSR_VEC) {
+		switch (h.desc.vec_len) {
+		case 1: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
+		case 2: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 2, false>;
+		case 4: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 4, false>;
+		case 8: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 8, false>;
+		case 16: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 16, false>;
+		}
+		return nullptr;
+	}
+	if (fmt == SPMV_FMT_SELL_SORTED)
+		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+	if (fmt == SPMV_FMT_SELL)
+		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+	return nullptr;
+}
+
+}  // namespace
+
+// Grid / shared-memory geometry of the staged kernel for this handle.
+int staged_geometry(Handle & h)
+{
+	const int cap_al = h.block_cap + 8;
+	const int stage_bytes = (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
+	// keep the pipeline inside the 227 KB a CTA may use (fewer stages for large blocks)
+	const int max_stages = (int) ((220 * 1024 - 64) / stage_bytes);
+	if (max_stages < 1) {
+		set_error(SPMV_ERR_ARG, "staging block of %d entries exceeds shared memory", h.block_cap);
+		return SPMV_ERR_ARG;
+	}
+	if (h.stages > max_stages)
+		h.stages = max_stages;
+	h.smem_bytes = (size_t) h.stages * stage_bytes + 64;
+	StagedFn kern = pick_staged(h);
+	if (!kern) {
+		set_error(SPMV_ERR_ARG, "no staged kernel for format %d with vec_len %d", h.desc.format, h.desc.vec_len);
+		return SPMV_ERR_ARG;
+	}
+	SPMV_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) h.smem_bytes));
+	int ctas = h.desc.ctas_per_sm > 0 ? h.desc.ctas_per_sm : 0;
+	if (ctas == 0) {
+		int per_sm = 0;
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STAGED_THREADS, h.smem_bytes));
+		ctas = per_sm > 0 ? per_sm : 1;
+	}
+	int64_t g = (int64_t) h.num_sms * ctas;
+	if (g > h.num_blocks)
+		g = h.num_blocks;
+	h.grid = (int) (g > 0 ? g : 1);
+	return SPMV_OK;
+}
+
+int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_DIV_RF)
+		return launch_div(h, d_x, d_y, s);
+	if (fmt == SPMV_FMT_SELL_C_S || ((fmt == SPMV_FMT_SELL || fmt == SPMV_FMT_SELL_SORTED) && h.desc.vec_len >= 32)) {
+		SlicedArgs a{};
+		a.x = d_x;
+		a.y = d_y;
+		a.m = h.m;
+		if (fmt == SPMV_FMT_SELL_C_S) {
+			a.sptr = h.d_sptr;
+			a.widths = h.d_widths;
+			a.cols = h.d_scols;
+			a.vals = h.d_svals;
+			a.ymap = h.d_order;
+			a.nslices = h.nslices;
+			a.C = h.desc.sellcs_c;
+		} else {
+			a.rcp = h.d_rcp;
+			a.cols = h.d_ja;
+			a.vals = h.d_a;
+			a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
+			a.nslices = h.nclusters;
+			a.C = h.desc.vec_len;
+		}
+		if (a.nslices == 0)
+			return SPMV_OK;
+		const int spc = 256 / a.C;
+		int64_t grid = ceil_div(a.nslices, spc);
+		const int64_t cap = (int64_t) h.num_sms * 16;
+		if (grid > cap)
+			grid = cap;
+		if (a.sptr) {
+			sliced_kernel<true, true><<<(unsigned) grid, 256, 0, s>>>(a);
+		} else if (a.ymap) {
+			sliced_kernel<false, true><<<(unsigned) grid, 256, 0, s>>>(a);
+		} else {
+			sliced_kernel<false, false><<<(unsigned) grid, 256, 0, s>>>(a);
+		}
+		SPMV_CUDA_TRY(cudaGetLastError());
+		return SPMV_OK;
+	}
+
+	if (h.num_blocks == 0)
+		return SPMV_OK;
+	StagedArgs a{};
+	a.blocks = h.d_blocks;
+	a.nblocks = h.num_blocks;
+	a.x = d_x;
+	a.y = d_y;
+	a.m = h.m;
+	a.cap_al = h.block_cap + 8;
+	a.stages = h.stages;
+	a.stage_bytes = (int) (ceil_div((int64_t) a.cap_al * 12, 128) * 128);
+	a.exact = h.desc.exact;
+	a.err = h.d_err;
+	if (fmt == SPMV_FMT_CSR_NAIVE || fmt == SPMV_FMT_CSR_VEC) {
+		a.ptr = h.d_rp;
+		a.cols = h.d_ci;
+		a.vals = h.d_v;
+	} else {
+		a.ptr = h.d_rcp;
+		a.cols = h.d_ja;
+		a.vals = h.d_a;
+		a.V = h.desc.vec_len;
+		a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
+	}
+	StagedFn kern = pick_staged(h);
+	kern<<<h.grid, STAGED_THREADS, h.smem_bytes, s>>>(a);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	return SPMV_OK;
+}
+
+}  // namespace spmv

@@ -1,0 +1,196 @@
+"""GPU parity: conversions and y through the C ABI against the reference's own outputs
+(golden fixtures) and the oracle restatement (full-size configs).
+
+Bars:
+  * every converted array (row_cluster_ptr, ja, a, permutations, thread ranges, row_order,
+    slice widths/pointers, columns, values) bit-identical;
+  * y bit-identical to the same format's reference y (each kernel sums a row in the
+    reference format's own order: csr_naive split multiply/add, csr_vec 4 FMA lanes,
+    sell / sell_sorted / sell_c_s one FMA per slice column);
+  * every format within 1e-12 per row of the reference csr_naive y, relative to
+    max(|y_i|, sum_j |a_ij x_j|) (the condition-aware tolerance).
+"""
+import numpy as np
+import pytest
+
+from conftest import assert_golden_array, golden_names, load_golden, rel_row_error
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+T, V = 8, 4
+REF_FORMATS = ["csr_naive", "csr_vec", "sell", "sell_sorted"]
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint64)
+
+
+def _eq_bits(a, b):
+    a, b = np.ascontiguousarray(a, np.float64), np.ascontiguousarray(b, np.float64)
+    bad = np.flatnonzero(_bits(a) != _bits(b))
+    return bad
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "the gpu tests need a CUDA device"
+    return torch
+
+
+def _mk(sb, g, fmt, **kw):
+    rp, ci, v = g["row_ptr"], g["col_ind"], g["values"]
+    return sb.csr_to_format(rp, ci, v, rp.size - 1, int(g["n"]), int(rp[-1]), format=fmt, **kw)
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("fmt", REF_FORMATS)
+def test_format_matches_reference(sb, orc, name, fmt):
+    g = load_golden(name)
+    mf = _mk(sb, g, fmt, num_threads=T, vec_len=V)
+    y = np.full(mf.m, 1.0)            # the reference's empty-row probe (bench_spmv.cpp:561-564)
+    mf.spmv(g["x"], y)
+    bad = _eq_bits(y, g[f"y_{fmt}"])
+    assert bad.size == 0, f"{fmt}/{name}: {bad.size} rows differ from the reference, first {bad[:5]}"
+    assert mf.mem_footprint == float(g[f"mem_{fmt}"])
+    if fmt in ("sell", "sell_sorted"):
+        keys = ["row_cluster_ptr", "ja", "a", "ranges"] + (["permutation", "rev_permutation"] if fmt == "sell_sorted" else [])
+        for k in keys:
+            assert_golden_array(g, f"{fmt}_{k}", mf.export(k))
+    gold, absy = orc.csr_gold(g["row_ptr"], g["col_ind"], g["values"], g["x"])
+    assert rel_row_error(y, g["y_csr_naive"], absy) <= TOL
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("C,sigma", [(32, 256), (64, 64)])
+def test_sellcs_matches_reference(sb, orc, name, C, sigma):
+    g = load_golden(name)
+    mf = _mk(sb, g, "sell_c_s", sellcs_c=C, sellcs_sigma=sigma)
+    pre = f"sellcs_{C}_{sigma}_"
+    assert_golden_array(g, pre + "row_order", mf.export("row_order").astype(np.int64))
+    assert_golden_array(g, pre + "slice_widths", mf.export("slice_widths").astype(np.int64))
+    assert_golden_array(g, pre + "slice_pointers", mf.export("slice_pointers"))
+    assert_golden_array(g, pre + "column_indices", mf.export("column_indices").astype(np.int64))
+    assert_golden_array(g, pre + "values", mf.export("sellcs_values"))
+    y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+    arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], C, sigma)
+    y_orc = orc.sellcs_spmv(arr, mf.m, C, g["x"])
+    assert _eq_bits(y, y_orc).size == 0
+    gold, absy = orc.csr_gold(g["row_ptr"], g["col_ind"], g["values"], g["x"])
+    assert rel_row_error(y, g["y_csr_naive"], absy) <= TOL
+
+
+@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s"])
+def test_device_path_equals_host_path(sb, torch_cuda, fmt):
+    torch = torch_cuda
+    g = load_golden("gen_gamma_skew_2000")
+    mf = _mk(sb, g, fmt)
+    y_host = mf.spmv(g["x"])
+    xd = torch.from_numpy(g["x"]).cuda()
+    yd = torch.full((mf.m,), 7.0, dtype=torch.float64, device="cuda")
+    mf.spmv(xd, yd)
+    torch.cuda.synchronize()
+    assert _eq_bits(yd.cpu().numpy(), y_host).size == 0
+
+
+@pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted"])
+@pytest.mark.parametrize("block_nnz,stages", [(64, 2), (256, 3), (8192, 4)])
+def test_staging_geometry_does_not_change_results(sb, fmt, block_nnz, stages):
+    """Tiny staging blocks force the long-unit path (rows / slices larger than a block)."""
+    for name in ["long_rows_60", "gen_gamma_skew_2000", "empty_rows_333"]:
+        g = load_golden(name)
+        mf = _mk(sb, g, fmt, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        assert _eq_bits(y, g[f"y_{fmt}"]).size == 0, (name, fmt, block_nnz)
+
+
+def test_non_exact_long_rows_within_tolerance(sb, orc):
+    g = load_golden("long_rows_60")
+    mf = _mk(sb, g, "csr_naive", exact=0, block_nnz=512)
+    y = mf.spmv(g["x"])
+    gold, absy = orc.csr_gold(g["row_ptr"], g["col_ind"], g["values"], g["x"])
+    assert rel_row_error(y, g["y_csr_naive"], absy) <= TOL
+
+
+@pytest.mark.parametrize("Vw", [32, 64])
+@pytest.mark.parametrize("fmt", ["sell", "sell_sorted"])
+def test_wide_slices_match_restatement(sb, orc, fmt, Vw):
+    g = load_golden("gen_diag_1500")
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf = _mk(sb, g, fmt, vec_len=Vw)
+    y = mf.spmv(x)
+    if fmt == "sell":
+        arr = orc.sell_convert(rp, ci, v, Vw, T)
+        y_orc = orc.sell_spmv(arr, mf.m, Vw, x)
+    else:
+        arr = orc.sell_sorted_convert(rp, ci, v, Vw, T)
+        y_orc = orc.sell_sorted_spmv(arr, mf.m, Vw, x)
+    for k in ["row_cluster_ptr", "ja", "a"]:
+        assert np.array_equal(mf.export(k).view(np.uint8), np.ascontiguousarray(arr[k]).view(np.uint8)), k
+    assert _eq_bits(y, y_orc).size == 0
+
+
+@pytest.mark.parametrize("threads", [1, 3, 64])
+@pytest.mark.parametrize("fmt", ["sell", "sell_sorted"])
+def test_thread_count_layouts(sb, orc, fmt, threads):
+    g = load_golden("empty_rows_333")
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf = _mk(sb, g, fmt, num_threads=threads)
+    conv = orc.sell_convert if fmt == "sell" else orc.sell_sorted_convert
+    arr = conv(rp, ci, v, V, threads)
+    for k in arr:
+        assert np.array_equal(mf.export(k), arr[k]), k
+
+
+# ------------------------------------------------------------------ edge cases
+def _rand_csr(m, n, seed, empty_frac=0.2, maxlen=9):
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(1, maxlen + 1, m)
+    lens[rng.random(m) < empty_frac] = 0
+    lens = np.minimum(lens, n)
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens] or [np.empty(0)]).astype(np.int32)
+    v = rng.uniform(-1, 1, int(rp[-1]))
+    return rp, ci, v
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (5, 3), (3, 5), (7, 1000), (1001, 17)])
+@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s"])
+def test_small_and_rectangular(sb, orc, fmt, m, n):
+    rp, ci, v = _rand_csr(m, n, m * 31 + n)
+    x = np.random.default_rng(1).uniform(-1, 1, n)
+    mf = sb.csr_to_format(rp, ci, v, m, n, int(rp[-1]), format=fmt)
+    y = mf.spmv(x, np.full(m, 1.0))
+    if fmt == "csr_naive":
+        ref = orc.csr_spmv(rp, ci, v, x)
+    elif fmt == "csr_vec":
+        ref = orc.csr_vec_spmv(rp, ci, v, x, V)
+    elif fmt == "sell":
+        ref = orc.sell_spmv(orc.sell_convert(rp, ci, v, V, T), m, V, x)
+    elif fmt == "sell_sorted":
+        ref = orc.sell_sorted_spmv(orc.sell_sorted_convert(rp, ci, v, V, T), m, V, x)
+    else:
+        ref = orc.sellcs_spmv(orc.sellcs_convert(rp, ci, v, 32, 512), m, 32, x)
+    assert _eq_bits(y, ref).size == 0
+
+
+@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s"])
+def test_all_rows_empty_and_no_entries(sb, fmt):
+    m, n = 50, 40
+    rp = np.zeros(m + 1, np.int32)
+    mf = sb.csr_to_format(rp, np.empty(0, np.int32), np.empty(0), m, n, 0, format=fmt)
+    y = mf.spmv(np.ones(n), np.full(m, 1.0))
+    assert np.all(y == 0.0)
+
+
+def test_malformed_csr_is_rejected(sb):
+    rp = np.array([0, 2, 1, 3], np.int32)
+    with pytest.raises(sb.SpmvError) as e:
+        sb.csr_to_format(rp, np.array([0, 1, 2], np.int32), np.ones(3), 3, 3, 3)
+    assert e.value.status == 2
+    rp = np.array([0, 1, 2], np.int32)
+    with pytest.raises(sb.SpmvError) as e:
+        sb.csr_to_format(rp, np.array([0, 9], np.int32), np.ones(2), 2, 3, 2)
+    assert e.value.status == 2

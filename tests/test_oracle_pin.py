@@ -1,0 +1,113 @@
+"""The oracle restatement is pinned against the reference's own outputs.
+
+* golden fixtures (tests/golden/, made by make_golden.py from the reference compiled from
+  its sources): every converted array and every y, bit for bit;
+* when the reference build is present (oracle/_ref/), the full config-1 matrix
+  (100k x 100k, nnz 999,475) as well.
+"""
+import numpy as np
+import pytest
+
+from conftest import assert_golden_array, golden_names, load_golden
+
+T, V = 8, 4
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint64)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_restatement_matches_reference_fixture(orc, name):
+    g = load_golden(name)
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    n = int(g["n"])
+    m = rp.size - 1
+    assert np.array_equal(_bits(orc.csr_spmv(rp, ci, v, x)), _bits(g["y_csr_naive"]))
+    assert np.array_equal(_bits(orc.csr_vec_spmv(rp, ci, v, x, V)), _bits(g["y_csr_vec"]))
+
+    s = orc.sell_convert(rp, ci, v, V, T)
+    for k in ["row_cluster_ptr", "ja", "a", "ranges"]:
+        assert_golden_array(g, f"sell_{k}", s[k])
+    assert np.array_equal(_bits(orc.sell_spmv(s, m, V, x)), _bits(g["y_sell"]))
+
+    s = orc.sell_sorted_convert(rp, ci, v, V, T)
+    for k in ["row_cluster_ptr", "ja", "a", "permutation", "rev_permutation", "ranges"]:
+        assert_golden_array(g, f"sell_sorted_{k}", s[k])
+    assert np.array_equal(_bits(orc.sell_sorted_spmv(s, m, V, x)), _bits(g["y_sell_sorted"]))
+
+    for C, sig in [(32, 256), (64, 64)]:
+        s = orc.sellcs_convert(rp, ci, v, C, sig)
+        for k in ["row_order", "slice_widths", "slice_pointers", "column_indices", "values"]:
+            assert_golden_array(g, f"sellcs_{C}_{sig}_{k}", s[k].astype(np.int64) if k != "values" else s[k])
+
+    d = orc.div_convert(rp, ci, v, n, T, V, 16384, 0.0)
+    assert_golden_array(g, "div_data", d["data"])
+    assert_golden_array(g, "div_group_pos", d["group_pos"])
+    assert_golden_array(g, "div_ranges", d["ranges"])
+    assert np.array_equal(_bits(orc.div_spmv(d, m, x, fused=True)), _bits(g["y_div_rf"]))
+
+    d = orc.div_convert(rp, ci, v, n, T, V, 1000, 0.0)
+    assert_golden_array(g, "div1000_data", d["data"])
+    assert_golden_array(g, "div1000_group_pos", d["group_pos"])
+    assert np.array_equal(_bits(orc.div_spmv(d, m, x, fused=True)), _bits(g["y_div_rf_1000"]))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_div_round_trip(orc, name):
+    """DIV-RF decodes back to the input matrix (the reference's self-check, div.cpp:515-603)."""
+    g = load_golden(name)
+    rp, ci, v = g["row_ptr"], g["col_ind"], g["values"]
+    m, nnz = rp.size - 1, int(rp[-1])
+    for pv in (16384, 1000, 7):
+        d = orc.div_convert(rp, ci, v, int(g["n"]), T, V, pv, 0.0)
+        r, c, val = orc.div_decode_coo(d["data"], V, nnz)
+        order = np.lexsort((c, r))
+        rows = np.repeat(np.arange(m), np.diff(rp))
+        assert np.array_equal(r[order], rows)
+        assert np.array_equal(c[order], ci)
+        assert np.array_equal(_bits(val[order]), _bits(v))
+
+
+def test_restatement_matches_reference_config1(orc):
+    """Config 1 at full size against the reference compiled from its sources."""
+    if not orc.ref_available("div_rf"):
+        pytest.skip("reference build (oracle/_ref) not present")
+    rp, ci, v, st = orc.ref_generate(100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14)
+    assert int(rp[-1]) == 999475
+    v = 2 * v - 1
+    m = rp.size - 1
+    x = np.random.default_rng(7).uniform(-1, 1, m)
+    for fmt in ["csr_naive", "sell", "sell_sorted", "div_rf"]:
+        R = orc.RefFormat(fmt, rp, ci, v, threads=T)
+        y = R.spmv(x)[:m]
+        if fmt == "csr_naive":
+            assert np.array_equal(_bits(orc.csr_spmv(rp, ci, v, x)), _bits(y))
+        elif fmt == "sell":
+            a, o = R.sell_arrays(), orc.sell_convert(rp, ci, v, V, T)
+            for k in a:
+                assert np.array_equal(a[k], o[k])
+            assert np.array_equal(_bits(orc.sell_spmv(o, m, V, x)), _bits(y))
+        elif fmt == "sell_sorted":
+            a, o = R.sell_arrays(), orc.sell_sorted_convert(rp, ci, v, V, T)
+            for k in a:
+                assert np.array_equal(a[k], o[k])
+        else:
+            a, o = R.div_arrays(), orc.div_convert(rp, ci, v, m, T, V, 16384, 0.0)
+            assert np.array_equal(a["data"], o["data"])
+            assert np.array_equal(_bits(orc.div_spmv(o, m, x, fused=True)), _bits(y))
+    for C, sig in [(32, 256), (256, 16384)]:
+        a, o = orc.ref_sellcs_convert(rp, ci, v, C, sig), orc.sellcs_convert(rp, ci, v, C, sig)
+        for k in a:
+            assert np.array_equal(a[k], o[k].astype(a[k].dtype))
+
+
+def test_partitioner_edge_cases(orc):
+    """Nearest-index balancing: equal prefix sums (empty rows), single element, T > N."""
+    sums = np.array([0, 0, 0, 5, 5, 5, 9, 20], np.int32)
+    got = [orc.partition_prefix_sums(4, t, sums, 7, 20) for t in range(4)]
+    assert got[0][0] == 0 and got[-1][1] == 7
+    for (s0, e0), (s1, e1) in zip(got, got[1:]):
+        assert e0 == s1
+    one = [orc.partition_prefix_sums(8, t, np.array([0, 3], np.int32), 1, 3) for t in range(8)]
+    assert one[0] == (0, 0) and one[-1] == (0, 1)
