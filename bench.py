@@ -132,6 +132,22 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class stdout_to_stderr:
+    """The reference's CPU code prints progress to stdout; keep stdout for the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -165,8 +181,15 @@ def max_over_ranks(world, v):
     return float(t.item())
 
 
-def generate(sb):
-    g = sb.generate_artificial(*CONFIG2)
+def config_tuple(args):
+    """Config 2, optionally with fewer rows/cols (--rows, for profiling captures)."""
+    if args.rows:
+        return (args.rows, args.rows) + CONFIG2[2:]
+    return CONFIG2
+
+
+def generate(sb, args):
+    g = sb.generate_artificial(*config_tuple(args))
     v = 2.0 * g.values - 1.0
     x = np.random.default_rng(12345).uniform(-1.0, 1.0, g.m)
     return g.row_ptr, g.col_ind, v, x
@@ -195,7 +218,7 @@ def run_ours(args):
     sb = load_package()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    rp, ci, v, x = generate(sb)
+    rp, ci, v, x = generate(sb, args)
     m, n, nnz = rp.size - 1, rp.size - 1, int(rp[-1])
     B = algorithmic_bytes(m, n, nnz)
     flops = 2.0 * nnz
@@ -265,7 +288,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (the reference's artificial generator restated natively, config 2; values 2v-1, x U[-1,1))",
-        "config": {"workload": WORKLOAD, "format": args.format, "m": m, "n": n, "nnz": nnz,
+        "config": {"workload": WORKLOAD if not args.rows else WORKLOAD.replace("4Mx4M", f"{m}x{n}"),
+                   "format": args.format, "m": m, "n": n, "nnz": nnz,
                    "bytes_per_spmv": B, "gflops": round(head["gflops"], 2),
                    "l2": "no flush: inputs (1.05 GB/SpMV) exceed the 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -282,7 +306,8 @@ def run_ours(args):
                        for k, r in per_format.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args.format, rp, ci, v, x, B, sample_s=args.cpu_seconds)
+        with stdout_to_stderr():
+            out["cpu_baseline"] = cpu_baseline(args.format, rp, ci, v, x, B, sample_s=args.cpu_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -330,21 +355,24 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": f"reference build oracle/_ref/libref_{name}.so missing"}))
         return
     cores = len(os.sched_getaffinity(0))
-    rp, ci, v, st = O.ref_generate(*CONFIG2[:4], CONFIG2[4], CONFIG2[5], *CONFIG2[6:10], CONFIG2[10], threads=cores)
+    cfg = config_tuple(args)
+    with stdout_to_stderr():
+        rp, ci, v, st = O.ref_generate(*cfg, threads=cores)
     v = 2.0 * v - 1.0
     m = n = rp.size - 1
     nnz = int(rp[-1])
     x = np.random.default_rng(12345).uniform(-1.0, 1.0, n)
     B = algorithmic_bytes(m, n, nnz)
-    R = O.RefFormat(name, rp, ci, v, threads=cores)
-    y = np.ones(m + 64)
-    for _ in range(args.warmup):
-        R.spmv(x, y)
-    per = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        R.spmv(x, y)
-        per.append(time.perf_counter() - t0)
+    with stdout_to_stderr():
+        R = O.RefFormat(name, rp, ci, v, threads=cores)
+        y = np.ones(m + 64)
+        for _ in range(args.warmup):
+            R.spmv(x, y)
+        per = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            R.spmv(x, y)
+            per.append(time.perf_counter() - t0)
     ms = 1e3 * sum(per) / len(per)
     val = B * 1e-9 / (ms * 1e-3)
     out = {
@@ -372,6 +400,7 @@ def main():
     ap.add_argument("--only-format", dest="all_formats", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--rows", type=int, default=0, help="config 2 with this many rows/cols (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

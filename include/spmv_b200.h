@@ -74,7 +74,12 @@ extern "C" {
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity).                   default 1
  *   values               SPMV_VALUES_F64 or SPMV_VALUES_F32.                       default F64
- *   block_nnz, block_rows, stages, ctas_per_sm: kernel tuning knobs, 0 = default.
+ *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
+ *                    staged per block, rows per block, pipeline depth, CTAs per SM,
+ *                    threads per CTA), 0 = default.
+ *   kernel           0: CTA staged kernel (bulk copy + shared-memory gather, every format);
+ *                    1: direct column-major kernel for slices of >= 32 rows;
+ *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows).  default 0
  */
 typedef struct spmv_format_desc {
 	int32_t format;
@@ -90,7 +95,9 @@ typedef struct spmv_format_desc {
 	int32_t block_rows;
 	int32_t stages;
 	int32_t ctas_per_sm;
-	int32_t reserved[8];
+	int32_t kernel;
+	int32_t threads;
+	int32_t reserved[6];
 } spmv_format_desc;
 
 typedef struct spmv_handle spmv_handle;

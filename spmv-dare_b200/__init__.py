@@ -85,6 +85,21 @@ def _is_cuda_tensor(a):
     return getattr(a, "is_cuda", False) is True
 
 
+CUDA_STREAM_LEGACY = 1   # cudaStreamLegacy: torch's default stream reports handle 0
+
+
+def _torch_stream(device, stream=None):
+    """Raw cudaStream_t of `stream` (a torch.cuda.Stream or raw handle) or of torch's current
+    stream.  The legacy default stream (handle 0) is passed as cudaStreamLegacy, because a
+    NULL stream means "the handle's own stream" in the C ABI."""
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+    return h if h else CUDA_STREAM_LEGACY
+
+
 class Matrix_Format:
     """A matrix converted to one GPU format (the reference's struct Matrix_Format)."""
 
@@ -131,7 +146,7 @@ class Matrix_Format:
                 raise ValueError("x and y must be contiguous")
             if x.numel() < self.n or y.numel() < self.m:
                 raise ValueError(f"x needs {self.n} and y {self.m} elements")
-            s = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
+            s = _torch_stream(x.device, stream)
             if x.dtype == torch.float32:
                 st = lib.spmv_run_device_f32(self._h, x.data_ptr(), y.data_ptr(), s)
             else:
@@ -222,7 +237,7 @@ def csr_to_format(row_ptr, col_ind, values, m=None, n=None, nnz=None, symmetric=
         if rp.dtype != torch.int32 or ci.dtype != torch.int32 or vv.dtype != torch.float64:
             raise TypeError("device CSR must be int32 row_ptr / col_ind and float64 values")
         h = lib.spmv_create_device(rp.data_ptr(), ci.data_ptr(), vv.data_ptr(), m, n, nnz, byref(desc),
-                                   torch.cuda.current_stream(rp.device).cuda_stream, byref(st))
+                                   _torch_stream(rp.device), byref(st))
     else:
         rp = _host(row_ptr, np.int32)
         ci = _host(col_ind, np.int32)

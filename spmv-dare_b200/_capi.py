@@ -50,7 +50,8 @@ class FormatDesc(ctypes.Structure):
         ("format", c_int32), ("num_threads", c_int32), ("vec_len", c_int32), ("sellcs_c", c_int32),
         ("sellcs_sigma", c_int32), ("div_packet_vals", c_int32), ("div_tolerance", c_double),
         ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
-        ("stages", c_int32), ("ctas_per_sm", c_int32), ("reserved", c_int32 * 8),
+        ("stages", c_int32), ("ctas_per_sm", c_int32), ("kernel", c_int32), ("threads", c_int32),
+        ("reserved", c_int32 * 6),
     ]
 
 

@@ -101,9 +101,18 @@ int build_blocks(Handle & h, const int32_t * d_P, int64_t U, int max_units)
 
 void staged_defaults(Handle & h)
 {
-	h.block_cap = h.desc.block_nnz > 0 ? h.desc.block_nnz : 2048;
+	// defaults measured on B200 with the 4M-row configuration (staging capacity, CTA size)
+	int cap = 1024, threads = 256;
+	if (h.desc.format == SPMV_FMT_CSR_NAIVE)
+		cap = 768;
+	else if (h.desc.format == SPMV_FMT_SELL_C_S) {
+		cap = 2048;
+		threads = 512;
+	}
+	h.block_cap = h.desc.block_nnz > 0 ? h.desc.block_nnz : cap;
 	h.block_cap = (h.block_cap + 7) & ~7;
-	h.stages = h.desc.stages > 0 ? h.desc.stages : 3;
+	h.stages = h.desc.stages > 0 ? h.desc.stages : 2;
+	h.threads = h.desc.threads > 0 ? h.desc.threads : threads;
 }
 
 // ------------------------------------------------------------------ SELL
@@ -398,11 +407,30 @@ int validate_csr(Handle & h)
 	return SPMV_OK;
 }
 
+// Kernel choice: the CTA staged kernel (0) by default; 1 = direct column-major kernel
+// (slices of >= 32 rows only), 2 = warp-autonomous staged kernel (slices of <= 32 rows).
+int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
+{
+	int k = h.desc.kernel;
+	if (k == 1 && V < 32)
+		k = 0;
+	if (k == 2 && V > 32)
+		k = 0;
+	h.exec_kernel = k;
+	if (k == 1)
+		return SPMV_OK;
+	if (k == 2)
+		return build_warp_chunks(h, d_P, U, V);
+	staged_defaults(h);
+	int max_units = (h.desc.block_rows > 0 ? h.desc.block_rows : h.threads) / V;
+	if (max_units < 1)
+		max_units = 1;
+	return build_blocks(h, d_P, U, max_units);
+}
+
 int convert_csr(Handle & h)
 {
-	staged_defaults(h);
-	int max_rows = h.desc.block_rows > 0 ? h.desc.block_rows : 1024;
-	return build_blocks(h, h.d_rp, h.m, max_rows);
+	return build_exec(h, h.d_rp, h.m, 1);
 }
 
 int convert_sell(Handle & h, bool sorted)
@@ -469,14 +497,7 @@ int convert_sell(Handle & h, bool sorted)
 		SPMV_TRY(sell_from_csr(h, rp2.as<int32_t>(), ci2.as<int32_t>(), v2.as<double>(), ranges.as<int64_t>()));
 		SPMV_CUDA_TRY(cudaStreamSynchronize(s));
 	}
-	if (V < 32) {
-		staged_defaults(h);
-		int max_slices = (h.desc.block_rows > 0 ? h.desc.block_rows : 1024) / V;
-		if (max_slices < 1)
-			max_slices = 1;
-		SPMV_TRY(build_blocks(h, h.d_rcp, nc, max_slices));
-	}
-	return SPMV_OK;
+	return build_exec(h, h.d_rcp, nc, V);
 }
 
 int convert_sellcs(Handle & h)
@@ -521,12 +542,19 @@ int convert_sellcs(Handle & h)
 	SPMV_TRY(h.alloc(&h.d_svals, total + 8));
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_scols, 0, (total + 8) * sizeof(int32_t), s));
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_svals, 0, (total + 8) * sizeof(double), s));
+	if (total > INT32_MAX - 64) {
+		set_error(SPMV_ERR_OVERFLOW, "SELL-C-sigma stores %lld entries, beyond the 32-bit range", (long long) total);
+		return SPMV_ERR_OVERFLOW;
+	}
+	SPMV_TRY(h.alloc(&h.d_sptr32, ns + 1));
+	i64_to_i32_kernel<<<(unsigned) ceil_div(ns + 1, 256), 256, 0, s>>>(h.d_sptr, h.d_sptr32, ns + 1);
+	SPMV_CUDA_TRY(cudaGetLastError());
 	if (ns > 0) {
 		sellcs_fill_kernel<<<(unsigned) ceil_div(ns * C, 256), 256, 0, s>>>(h.d_rp, h.d_ci, h.d_v, h.d_order, m, C, ns,
 				h.d_widths, h.d_sptr, h.d_scols, h.d_svals);
 		SPMV_CUDA_TRY(cudaGetLastError());
 	}
-	return SPMV_OK;
+	return build_exec(h, h.d_sptr32, ns, C);
 }
 
 }  // namespace spmv

@@ -19,6 +19,18 @@ struct StagedBlock {
 	int32_t elems;
 };
 
+// A chunk of the warp-autonomous kernel: units [unit0, unit0 + units) (rows, or slices of
+// V rows) whose entries [elem0, elem0 + elems) are staged together.  A unit larger than
+// one chunk spans consecutive chunks with flags 1 (continues the previous chunk) and
+// 2 (continues in the next chunk).
+struct WarpChunk {
+	int32_t unit0;
+	uint16_t units;
+	uint16_t flags;
+	int32_t elem0;
+	int32_t elems;
+};
+
 enum class Kind { CSR = 0, SLICED = 1 };
 enum class Arith { SEQ_SPLIT = 0, SEQ_FMA = 1, LANES_FMA = 2 };
 
@@ -42,7 +54,16 @@ struct Handle {
 	int grid = 0;
 	int block_cap = 0;           // staging capacity in entries
 	int stages = 0;
+	int threads = 256;           // threads per CTA of the staged kernel
 	size_t smem_bytes = 0;
+	int exec_kernel = 0;         // 0 CTA staged, 1 direct sliced, 2 warp-autonomous
+
+	// warp-autonomous kernel
+	WarpChunk * d_chunks = nullptr;
+	int64_t num_chunks = 0;
+	int32_t * d_warp_begin = nullptr;
+	int64_t num_warps = 0;
+	int warp_bytes = 0;
 
 	// SELL / sell_sorted (slice height V)
 	int64_t nclusters = 0;
@@ -60,6 +81,7 @@ struct Handle {
 	int32_t * d_order = nullptr;
 	int32_t * d_widths = nullptr;
 	int64_t * d_sptr = nullptr;
+	int32_t * d_sptr32 = nullptr;   // the same slice pointers, 32-bit, for the staged kernel
 	int32_t * d_scols = nullptr;
 	double * d_svals = nullptr;
 
@@ -114,9 +136,12 @@ int convert_sell(Handle & h, bool sorted);
 int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
 
-// ---- staged-block construction over a CSR row pointer or a slice pointer
-int build_csr_blocks(Handle & h, const int32_t * d_rowptr, int64_t rows);
-int build_slice_blocks(Handle & h, const int32_t * d_sliceptr, int64_t slices, int V);
+
+// Builds the execution schedule of the chosen kernel over the unit pointer P (CSR row_ptr
+// with V = 1, or a slice pointer with slice height V).
+int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V);
+int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V);
+int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
 
 // ---- SpMV launches
 int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s);

@@ -24,7 +24,7 @@ namespace spmv {
 
 namespace {
 
-constexpr int STAGED_THREADS = 256;
+constexpr int STAGED_MAX_THREADS = 512;
 
 struct StagedArgs {
 	const StagedBlock * blocks;
@@ -132,12 +132,107 @@ __device__ __forceinline__ double cta_sum(double v, double * red)
 	return t;
 }
 
+// Long unit (a row / slice larger than one staged block) streamed through the gather
+// buffer in chunks; every row is still summed by one thread in the reference order.
 template <Kind K, Arith A, int L, bool YMAP>
-__global__ void __launch_bounds__(STAGED_THREADS) staged_kernel(StagedArgs a)
+__device__ __forceinline__ void staged_long_unit(const StagedArgs & a, const StagedBlock & d, double * xb)
+{
+	const int half = a.cap_al / 2;            // entries per chunk: values in xb[0,half), x in xb[half, 2 half)
+	double * cv = xb;
+	double * cx = xb + half;
+	if (K == Kind::CSR && !a.exact) {
+		// tolerance mode: every thread a strided partial, then a fixed-order CTA sum
+		const int64_t r = d.unit0;
+		double part = 0.0;
+		for (int64_t j = a.ptr[r] + threadIdx.x; j < a.ptr[r + 1]; j += blockDim.x)
+			part = __fma_rn(a.vals[j], ldg(a.x + a.cols[j]), part);
+		double t = cta_sum(part, cv);
+		if (threadIdx.x == 0)
+			a.y[r] = t;
+		return;
+	}
+	if (K == Kind::CSR) {
+		const int64_t r = d.unit0;
+		const int64_t js = a.ptr[r], je = a.ptr[r + 1];
+		const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
+		double sum = 0.0;
+		double lane[L];
+		#pragma unroll
+		for (int l = 0; l < L; l++)
+			lane[l] = 0.0;
+		for (int64_t c0 = js; c0 < je; c0 += half) {
+			const int cnt = (int) ((je - c0) < half ? (je - c0) : half);
+			for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+				const double v = a.vals[c0 + e];
+				const double xv = ldg(a.x + a.cols[c0 + e]);
+				cv[e] = v;
+				cx[e] = xv;
+			}
+			__syncthreads();
+			if (threadIdx.x == 0) {
+				for (int e = 0; e < cnt; e++) {
+					const int64_t j = c0 + e;
+					if (A == Arith::LANES_FMA) {
+						if (j < jv) {
+							const int l = (int) ((j - js) & (L - 1));
+							#pragma unroll
+							for (int q = 0; q < L; q++)
+								if (q == l)
+									lane[q] = __fma_rn(cv[e], cx[e], lane[q]);
+						} else {
+							if (j == jv)
+								sum = lanes_reduce<L>(lane);
+							sum = __dadd_rn(sum, __dmul_rn(cv[e], cx[e]));
+						}
+					} else if (A == Arith::SEQ_FMA) {
+						sum = __fma_rn(cv[e], cx[e], sum);
+					} else {
+						sum = __dadd_rn(sum, __dmul_rn(cv[e], cx[e]));
+					}
+				}
+			}
+			__syncthreads();
+		}
+		if (threadIdx.x == 0) {
+			if (A == Arith::LANES_FMA && jv == je)
+				sum = lanes_reduce<L>(lane);
+			a.y[r] = sum;
+		}
+	} else {
+		const int V = a.V;
+		const int64_t sl = d.unit0;
+		const int64_t p0 = a.ptr[sl];
+		const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+		const int kc = half / V > 0 ? half / V : 1;     // slice columns per chunk
+		double acc = 0.0;
+		for (int k0 = 0; k0 < w; k0 += kc) {
+			const int kn = (w - k0) < kc ? (w - k0) : kc;
+			const int cnt = kn * V;
+			const int64_t base = p0 + (int64_t) k0 * V;
+			for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+				cv[e] = a.vals[base + e];
+				cx[e] = ldg(a.x + a.cols[base + e]);
+			}
+			__syncthreads();
+			if (threadIdx.x < V)
+				for (int k = 0; k < kn; k++)
+					acc = __fma_rn(cv[k * V + threadIdx.x], cx[k * V + threadIdx.x], acc);
+			__syncthreads();
+		}
+		if (threadIdx.x < V) {
+			const int64_t row = sl * V + threadIdx.x;
+			if (row < a.m)
+				a.y[YMAP ? a.ymap[row] : row] = acc;
+		}
+	}
+}
+
+template <Kind K, Arith A, int L, bool YMAP>
+__global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
-	__shared__ double red[STAGED_THREADS / 32];
-	uint64_t * bars = reinterpret_cast<uint64_t *>(smem + (size_t) a.stages * a.stage_bytes);
+	double * xb = reinterpret_cast<double *>(smem + (size_t) a.stages * a.stage_bytes);
+	uint64_t * bars = reinterpret_cast<uint64_t *>(smem + (size_t) a.stages * a.stage_bytes + (size_t) a.cap_al * 8);
 
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < a.stages; s++)
@@ -166,13 +261,59 @@ __global__ void __launch_bounds__(STAGED_THREADS) staged_kernel(StagedArgs a)
 		}
 		if (d.units >= 0) {
 			const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
-			const double * sv = reinterpret_cast<const double *>(smem + (size_t) s * a.stage_bytes);
+			const int off = (int) (d.elem0 - e0);
+			const int cnt = d.elems;
+			double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
 			const int32_t * sc = reinterpret_cast<const int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+			// row bounds of this thread's first row, loaded before the gather so their
+			// latency overlaps it
+			int js0 = 0, je0 = 0;
+			if (K == Kind::CSR && (int) threadIdx.x < d.units) {
+				const int64_t r = (int64_t) d.unit0 + threadIdx.x;
+				js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+				je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+			}
+			// 1) gather x for every staged entry, all threads, many loads in flight
+			#pragma unroll 4
+			for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+				const double xv = ldg(a.x + sc[off + e]);
+				if (A == Arith::SEQ_SPLIT)
+					sv[off + e] = __dmul_rn(sv[off + e], xv);   // the reference's rounded product
+				else
+					xb[off + e] = xv;
+			}
+			__syncthreads();
+			// 2) one thread per row, reference order, operands in shared memory
 			if (K == Kind::CSR) {
 				for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
 					const int64_t r = (int64_t) d.unit0 + u;
-					const int64_t js = (int64_t) a.ptr[r] - e0, je = (int64_t) a.ptr[r + 1] - e0;
-					a.y[r] = csr_row<A, L>(sv, sc, js, je, a.x);
+					const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
+					const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
+					double sum = 0.0;
+					if (A == Arith::SEQ_SPLIT) {
+						#pragma unroll 4
+						for (int j = js; j < je; j++)
+							sum = __dadd_rn(sum, sv[j]);
+					} else if (A == Arith::SEQ_FMA) {
+						#pragma unroll 4
+						for (int j = js; j < je; j++)
+							sum = __fma_rn(sv[j], xb[j], sum);
+					} else {
+						double ln[L];
+						#pragma unroll
+						for (int l = 0; l < L; l++)
+							ln[l] = 0.0;
+						const int jv = js + ((je - js) & ~(L - 1));
+						for (int j = js; j < jv; j += L) {
+							#pragma unroll
+							for (int l = 0; l < L; l++)
+								ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
+						}
+						sum = lanes_reduce<L>(ln);
+						for (int j = jv; j < je; j++)
+							sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
+					}
+					a.y[r] = sum;
 				}
 			} else {
 				const int V = a.V;
@@ -183,47 +324,17 @@ __global__ void __launch_bounds__(STAGED_THREADS) staged_kernel(StagedArgs a)
 					const int64_t row = sl * V + lane;
 					if (row >= a.m)
 						continue;
-					const int64_t ks = (int64_t) a.ptr[sl] - e0 + lane;
+					const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
 					const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
 					double acc = 0.0;
 					#pragma unroll 4
 					for (int k = 0; k < w; k++)
-						acc = __fma_rn(sv[ks + (int64_t) k * V], ldg(a.x + sc[ks + (int64_t) k * V]), acc);
+						acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
 					a.y[YMAP ? a.ymap[row] : row] = acc;
 				}
 			}
 		} else {
-			// A unit larger than the staging capacity, straight from global memory.
-			if (K == Kind::CSR) {
-				const int64_t r = d.unit0;
-				const int64_t js = a.ptr[r], je = a.ptr[r + 1];
-				if (a.exact) {
-					if (threadIdx.x == 0)
-						a.y[r] = csr_row<A, L>(a.vals, a.cols, js, je, a.x);
-				} else {
-					double part = 0.0;
-					for (int64_t j = js + threadIdx.x; j < je; j += blockDim.x)
-						part = __fma_rn(a.vals[j], ldg(a.x + a.cols[j]), part);
-					double t = cta_sum(part, red);
-					if (threadIdx.x == 0)
-						a.y[r] = t;
-				}
-			} else {
-				const int V = a.V;
-				const int64_t sl = d.unit0;
-				const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
-				for (int lane = threadIdx.x; lane < V; lane += blockDim.x) {
-					const int64_t row = sl * V + lane;
-					if (row >= a.m)
-						continue;
-					double acc = 0.0;
-					for (int k = 0; k < w; k++) {
-						const int64_t q = (int64_t) a.ptr[sl] + (int64_t) k * V + lane;
-						acc = __fma_rn(a.vals[q], ldg(a.x + a.cols[q]), acc);
-					}
-					a.y[YMAP ? a.ymap[row] : row] = acc;
-				}
-			}
+			staged_long_unit<K, A, L, YMAP>(a, d, xb);
 		}
 		__syncthreads();
 		if (threadIdx.x == 0) {
@@ -309,7 +420,7 @@ StagedFn pick_staged(const Handle & h)
 		}
 		return nullptr;
 	}
-	if (fmt == SPMV_FMT_SELL_SORTED)
+	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
 		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
 	if (fmt == SPMV_FMT_SELL)
 		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
@@ -324,14 +435,15 @@ int staged_geometry(Handle & h)
 	const int cap_al = h.block_cap + 8;
 	const int stage_bytes = (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
 	// keep the pipeline inside the 227 KB a CTA may use (fewer stages for large blocks)
-	const int max_stages = (int) ((220 * 1024 - 64) / stage_bytes);
+	const int xbuf_bytes = cap_al * 8;
+	const int max_stages = (int) ((220 * 1024 - 64 - xbuf_bytes) / stage_bytes);
 	if (max_stages < 1) {
 		set_error(SPMV_ERR_ARG, "staging block of %d entries exceeds shared memory", h.block_cap);
 		return SPMV_ERR_ARG;
 	}
 	if (h.stages > max_stages)
 		h.stages = max_stages;
-	h.smem_bytes = (size_t) h.stages * stage_bytes + 64;
+	h.smem_bytes = (size_t) h.stages * stage_bytes + (size_t) xbuf_bytes + 64;
 	StagedFn kern = pick_staged(h);
 	if (!kern) {
 		set_error(SPMV_ERR_ARG, "no staged kernel for format %d with vec_len %d", h.desc.format, h.desc.vec_len);
@@ -341,7 +453,7 @@ int staged_geometry(Handle & h)
 	int ctas = h.desc.ctas_per_sm > 0 ? h.desc.ctas_per_sm : 0;
 	if (ctas == 0) {
 		int per_sm = 0;
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STAGED_THREADS, h.smem_bytes));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h.threads, h.smem_bytes));
 		ctas = per_sm > 0 ? per_sm : 1;
 	}
 	int64_t g = (int64_t) h.num_sms * ctas;
@@ -356,7 +468,9 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	const int fmt = h.desc.format;
 	if (fmt == SPMV_FMT_DIV_RF)
 		return launch_div(h, d_x, d_y, s);
-	if (fmt == SPMV_FMT_SELL_C_S || ((fmt == SPMV_FMT_SELL || fmt == SPMV_FMT_SELL_SORTED) && h.desc.vec_len >= 32)) {
+	if (h.exec_kernel == 2)
+		return launch_warp(h, d_x, d_y, s);
+	if (h.exec_kernel == 1) {
 		SlicedArgs a{};
 		a.x = d_x;
 		a.y = d_y;
@@ -412,6 +526,12 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.ptr = h.d_rp;
 		a.cols = h.d_ci;
 		a.vals = h.d_v;
+	} else if (fmt == SPMV_FMT_SELL_C_S) {
+		a.ptr = h.d_sptr32;
+		a.cols = h.d_scols;
+		a.vals = h.d_svals;
+		a.V = h.desc.sellcs_c;
+		a.ymap = h.d_order;
 	} else {
 		a.ptr = h.d_rcp;
 		a.cols = h.d_ja;
@@ -420,7 +540,7 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
 	}
 	StagedFn kern = pick_staged(h);
-	kern<<<h.grid, STAGED_THREADS, h.smem_bytes, s>>>(a);
+	kern<<<h.grid, h.threads, h.smem_bytes, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;
 }

@@ -1,0 +1,513 @@
+// Warp-autonomous staged SpMV (the default kernel of the CSR and narrow-SELL formats).
+//
+// Every warp owns a contiguous run of "chunks" of the matrix and its own pipeline in
+// shared memory: a ring of bulk-copy stages (cp.async.bulk global->shared, completion on a
+// per-warp mbarrier), a gather buffer, and no CTA-wide barrier at all -- a warp waits only
+// for its own copies and its own 32 rows.  Per chunk:
+//   1. the chunk's stored entries (values, columns: one contiguous range) have landed;
+//   2. the 32 lanes gather x for every entry (coalesced when a row's columns are clustered)
+//      -- csr_naive stores the rounded product v*x in place, the FMA formats keep x;
+//   3. lane r sums its row (or slice lane) from shared memory in the reference format's
+//      own operation order, so y is bit-identical to the reference;
+//   4. lane 0 refills the stage with the chunk `stages` ahead.
+// A row / slice larger than one chunk spans consecutive chunks of the same warp and its
+// accumulators live in registers across them (flags CONT_PREV / CONT_NEXT).
+#include "internal.h"
+#include "primitives.cuh"
+
+namespace spmv {
+
+namespace {
+
+constexpr int WARP_CTA_THREADS = 128;         // 4 independent warps per CTA
+constexpr uint32_t CONT_PREV = 1, CONT_NEXT = 2;
+
+struct WarpArgs {
+	const WarpChunk * chunks;
+	const int32_t * warp_begin;    // chunk range of warp w: [warp_begin[w], warp_begin[w+1])
+	int64_t nwarps;
+	const int32_t * ptr;           // CSR row_ptr or slice pointer
+	const int32_t * cols;
+	const double * vals;
+	const int32_t * ymap;
+	const double * x;
+	double * y;
+	int64_t m;
+	int V;
+	int cap_al;                    // entries per stage buffer
+	int stages;
+	int stage_bytes;
+	int warp_bytes;                // shared memory per warp
+	int xbuf_bytes;                // gather buffer per warp (0 when products are stored in place)
+	int * err;
+};
+
+template <int L>
+__device__ __forceinline__ double lanes_reduce_w(const double * s)
+{
+	if (L == 1)
+		return s[0];
+	if (L == 2)
+		return s[0] + s[1];
+	if (L == 4)
+		return (s[0] + s[2]) + (s[1] + s[3]);
+	double tot = 0;
+	#pragma unroll
+	for (int h = 0; h < L; h += 4)
+		tot = tot + ((s[h] + s[h + 2]) + (s[h + 1] + s[h + 3]));
+	return tot;
+}
+
+__device__ __forceinline__ void warp_issue(const WarpArgs & a, int64_t c, uint8_t * wsm, uint64_t * bar, int s)
+{
+	const WarpChunk d = a.chunks[c];
+	if (d.elems == 0) {
+		mbar_arrive(bar);
+		return;
+	}
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	double * sv = reinterpret_cast<double *>(wsm + (size_t) s * a.stage_bytes);
+	int32_t * sc = reinterpret_cast<int32_t *>(wsm + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(bar, cnt * 12u);
+	bulk_g2s(sv, a.vals + e0, cnt * 8u, bar);
+	bulk_g2s(sc, a.cols + e0, cnt * 4u, bar);
+}
+
+template <Kind K, Arith A, int L, bool YMAP>
+__global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const int64_t w = (int64_t) blockIdx.x * (blockDim.x >> 5) + wib;
+	uint8_t * wsm = smem + (size_t) wib * a.warp_bytes;
+	double * xb = reinterpret_cast<double *>(wsm + (size_t) a.stages * a.stage_bytes);
+	uint64_t * bars = reinterpret_cast<uint64_t *>(wsm + (size_t) a.stages * a.stage_bytes + (size_t) a.xbuf_bytes);
+	if (w >= a.nwarps)
+		return;
+	const int64_t cb = a.warp_begin[w], ce = a.warp_begin[w + 1];
+	if (cb >= ce)
+		return;
+	if (lane == 0) {
+		for (int s = 0; s < a.stages; s++)
+			mbar_init(&bars[s], 1);
+		mbar_fence_init();
+	}
+	__syncwarp();
+	if (lane == 0)
+		for (int s = 0; s < a.stages && cb + s < ce; s++)
+			warp_issue(a, cb + s, wsm, &bars[s], s);
+
+	double acc = 0.0;          // a lane's running sum across chunks of one long unit
+	double ln[L];
+	#pragma unroll
+	for (int l = 0; l < L; l++)
+		ln[l] = 0.0;
+	int it = 0;
+	for (int64_t c = cb; c < ce; c++, it++) {
+		const int s = it % a.stages;
+		const uint32_t parity = (uint32_t) ((it / a.stages) & 1);
+		const WarpChunk d = a.chunks[c];
+		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
+		if (!__all_sync(0xffffffffu, ok)) {
+			if (lane == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		const int off = (int) (d.elem0 - e0);
+		double * sv = reinterpret_cast<double *>(wsm + (size_t) s * a.stage_bytes) + off;
+		const int32_t * sc = reinterpret_cast<const int32_t *>(wsm + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8) + off;
+		double * xs = xb + off;
+		// gather x for all entries of the chunk
+		#pragma unroll 8
+		for (int e = lane; e < d.elems; e += 32) {
+			const double xv = ldg(a.x + sc[e]);
+			if (A == Arith::SEQ_SPLIT)
+				sv[e] = __dmul_rn(sv[e], xv);
+			else
+				xs[e] = xv;
+		}
+		__syncwarp();
+		const bool long_unit = (d.flags & (CONT_PREV | CONT_NEXT)) != 0;
+		if (K == Kind::CSR) {
+			if (!long_unit) {
+				if (lane < d.units) {
+					const int64_t r = (int64_t) d.unit0 + lane;
+					const int js = a.ptr[r] - d.elem0, je = a.ptr[r + 1] - d.elem0;
+					double sum = 0.0;
+					if (A == Arith::SEQ_SPLIT) {
+						#pragma unroll 4
+						for (int j = js; j < je; j++)
+							sum = __dadd_rn(sum, sv[j]);
+					} else if (A == Arith::SEQ_FMA) {
+						#pragma unroll 4
+						for (int j = js; j < je; j++)
+							sum = __fma_rn(sv[j], xs[j], sum);
+					} else {
+						double q[L];
+						#pragma unroll
+						for (int l = 0; l < L; l++)
+							q[l] = 0.0;
+						const int jv = js + ((je - js) & ~(L - 1));
+						for (int j = js; j < jv; j += L) {
+							#pragma unroll
+							for (int l = 0; l < L; l++)
+								q[l] = __fma_rn(sv[j + l], xs[j + l], q[l]);
+						}
+						sum = lanes_reduce_w<L>(q);
+						for (int j = jv; j < je; j++)
+							sum = __dadd_rn(sum, __dmul_rn(sv[j], xs[j]));
+					}
+					a.y[r] = sum;
+				}
+			} else if (A == Arith::LANES_FMA) {
+				// one long row, csr_vec order: lane l < L keeps accumulator l (entries j with
+				// (j - row start) % L == l below the vector bound), lane 0 adds the tail
+				const int64_t r = d.unit0;
+				const int64_t js = a.ptr[r], je = a.ptr[r + 1];
+				const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
+				if (!(d.flags & CONT_PREV)) {
+					acc = 0.0;
+					ln[0] = 0.0;
+				}
+				if (lane < L) {
+					for (int e = 0; e < d.elems; e++) {
+						const int64_t j = (int64_t) d.elem0 + e;
+						if (j < jv && (int) ((j - js) & (L - 1)) == lane)
+							ln[0] = __fma_rn(sv[e], xs[e], ln[0]);
+					}
+				}
+				if (!(d.flags & CONT_NEXT) || (int64_t) d.elem0 + d.elems > jv) {
+					// the lane sums are final once the chunk passes the vector bound
+					double q[L];
+					#pragma unroll
+					for (int l = 0; l < L; l++)
+						q[l] = __shfl_sync(0xffffffffu, ln[0], l);
+					if (lane == 0) {
+						if ((int64_t) d.elem0 <= jv)
+							acc = lanes_reduce_w<L>(q);
+						for (int e = 0; e < d.elems; e++) {
+							const int64_t j = (int64_t) d.elem0 + e;
+							if (j >= jv)
+								acc = __dadd_rn(acc, __dmul_rn(sv[e], xs[e]));
+						}
+						if (!(d.flags & CONT_NEXT))
+							a.y[r] = acc;
+					}
+				}
+			} else if (lane == 0) {
+				// one long row: lane 0 continues the row's sum in the reference order
+				const int64_t r = d.unit0;
+				if (!(d.flags & CONT_PREV))
+					acc = 0.0;
+				for (int e = 0; e < d.elems; e++) {
+					if (A == Arith::SEQ_SPLIT)
+						acc = __dadd_rn(acc, sv[e]);
+					else
+						acc = __fma_rn(sv[e], xs[e], acc);
+				}
+				if (!(d.flags & CONT_NEXT))
+					a.y[r] = acc;
+			}
+		} else {
+			const int V = a.V;
+			if (!long_unit) {
+				if (lane < d.units * V) {
+					const int64_t sl = (int64_t) d.unit0 + lane / V;
+					const int r = lane % V;
+					const int64_t row = sl * V + r;
+					if (row < a.m) {
+						const int ks = a.ptr[sl] - d.elem0 + r;
+						const int wd = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+						double sum = 0.0;
+						#pragma unroll 4
+						for (int k = 0; k < wd; k++)
+							sum = __fma_rn(sv[ks + k * V], xs[ks + k * V], sum);
+						a.y[YMAP ? a.ymap[row] : row] = sum;
+					}
+				}
+			} else if (lane < V) {
+				// one long slice in column chunks: lane r continues row r of the slice
+				if (!(d.flags & CONT_PREV))
+					acc = 0.0;
+				const int kn = d.elems / V;
+				for (int k = 0; k < kn; k++)
+					acc = __fma_rn(sv[k * V + lane], xs[k * V + lane], acc);
+				if (!(d.flags & CONT_NEXT)) {
+					const int64_t row = (int64_t) d.unit0 * V + lane;
+					if (row < a.m)
+						a.y[YMAP ? a.ymap[row] : row] = acc;
+				}
+			}
+		}
+		__syncwarp();
+		if (lane == 0 && c + a.stages < ce)
+			warp_issue(a, c + a.stages, wsm, &bars[s], s);
+	}
+}
+
+using WarpFn = void (*)(WarpArgs);
+
+WarpFn pick_warp(const Handle & h)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_CSR_NAIVE)
+		return warp_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+	if (fmt == SPMV_FMT_CSR_VEC) {
+		switch (h.desc.vec_len) {
+		case 1: return warp_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
+		case 2: return warp_kernel<Kind::CSR, Arith::LANES_FMA, 2, false>;
+		case 4: return warp_kernel<Kind::CSR, Arith::LANES_FMA, 4, false>;
+		case 8: return warp_kernel<Kind::CSR, Arith::LANES_FMA, 8, false>;
+		case 16: return warp_kernel<Kind::CSR, Arith::LANES_FMA, 16, false>;
+		}
+		return nullptr;
+	}
+	if (fmt == SPMV_FMT_SELL)
+		return warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
+		return warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+	return nullptr;
+}
+
+// ------------------------------------------------------------------ chunk table
+constexpr int TILE_UNITS = 1024;
+
+// Chunks of one tile of units: normal chunks pack whole units (at most 32 rows and `cap`
+// entries); a unit larger than `cap` is cut into consecutive chunks (CSR: runs of entries;
+// slices: runs of whole slice columns) flagged CONT_PREV / CONT_NEXT.
+template <bool WRITE>
+__global__ void warp_chunks_kernel(const int32_t * P, int64_t U, int V, int cap, int64_t * counts, const int64_t * offs,
+		WarpChunk * out)
+{
+	int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	int64_t u = t * TILE_UNITS;
+	if (u >= U)
+		return;
+	const int64_t end = u + TILE_UNITS < U ? u + TILE_UNITS : U;
+	const int max_units = 32 / V;
+	int64_t nb = 0;
+	const int64_t o = WRITE ? offs[t] : 0;
+	while (u < end) {
+		const int64_t len = (int64_t) P[u + 1] - P[u];
+		if (len > cap) {
+			const int64_t step = (V == 1) ? cap : (int64_t) (cap / V) * V;
+			for (int64_t c0 = 0; c0 < len; c0 += step) {
+				const int64_t cl = (len - c0) < step ? (len - c0) : step;
+				if (WRITE) {
+					WarpChunk d;
+					d.unit0 = (int32_t) u;
+					d.units = 1;
+					d.flags = (uint16_t) ((c0 > 0 ? CONT_PREV : 0) | (c0 + cl < len ? CONT_NEXT : 0));
+					d.elem0 = (int32_t) (P[u] + c0);
+					d.elems = (int32_t) cl;
+					out[o + nb] = d;
+				}
+				nb++;
+			}
+			u++;
+			continue;
+		}
+		const int64_t start = u;
+		const int64_t e0 = P[u];
+		while (u < end && u - start < max_units && (int64_t) P[u + 1] - e0 <= cap)
+			u++;
+		if (WRITE) {
+			WarpChunk d;
+			d.unit0 = (int32_t) start;
+			d.units = (uint16_t) (u - start);
+			d.flags = 0;
+			d.elem0 = (int32_t) e0;
+			d.elems = (int32_t) ((int64_t) P[u] - e0);
+			out[o + nb] = d;
+		}
+		nb++;
+	}
+	if (!WRITE)
+		counts[t] = nb;
+}
+
+// Work estimate of a chunk: the bytes it stages plus a fixed cost; a chunk of a long unit
+// is summed by one lane (or the V lanes of a slice) in a dependent chain, so its entries
+// cost as much as LONG_FACTOR parallel ones -- long rows are spread over many warps.
+constexpr int64_t LONG_FACTOR = 24;
+
+__global__ void chunk_weights_kernel(const WarpChunk * ch, int64_t n, int V, int64_t * wgt)
+{
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const WarpChunk d = ch[i];
+	int64_t w = (int64_t) d.elems * 12 + 64;
+	if (d.flags & (CONT_PREV | CONT_NEXT))
+		w = (int64_t) d.elems * 12 * LONG_FACTOR / (V < 32 ? V : 32) + 64;
+	wgt[i] = w;
+}
+
+// Warp w starts at the first chunk whose weight prefix reaches w/W of the total and which
+// does not continue a previous chunk (long units stay with one warp).
+__global__ void warp_ranges_kernel(const WarpChunk * ch, const int64_t * prefix, int64_t n, int64_t W, int32_t * begin)
+{
+	int64_t w = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (w > W)
+		return;
+	if (w == 0) {
+		begin[0] = 0;
+		return;
+	}
+	if (w == W) {
+		begin[W] = (int32_t) n;
+		return;
+	}
+	const int64_t total = prefix[n];
+	const int64_t target = (total * w) / W;
+	int64_t lo = 0, hi = n;
+	while (lo < hi) {
+		int64_t mid = (lo + hi) >> 1;
+		if (prefix[mid] < target)
+			lo = mid + 1;
+		else
+			hi = mid;
+	}
+	while (lo < n && (ch[lo].flags & CONT_PREV))
+		lo++;
+	begin[w] = (int32_t) lo;
+}
+
+}  // namespace
+
+int warp_geometry(Handle & h)
+{
+	// fit 4 warps' pipelines in a CTA's shared memory: fewer stages, then a smaller chunk
+	for (;;) {
+		const int cap_al = h.block_cap + 8;
+		const int stage_bytes = (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
+		const int xbuf = (h.desc.format == SPMV_FMT_CSR_NAIVE) ? 0 : cap_al * 8;
+		h.warp_bytes = (int) (ceil_div((int64_t) h.stages * stage_bytes + xbuf + 8 * h.stages, 128) * 128);
+		h.smem_bytes = (size_t) h.warp_bytes * (WARP_CTA_THREADS / 32);
+		if (h.smem_bytes <= 220 * 1024)
+			break;
+		if (h.stages > 2)
+			h.stages--;
+		else if (h.block_cap > 64)
+			h.block_cap = ((h.block_cap / 2) + 7) & ~7;
+		else {
+			set_error(SPMV_ERR_ARG, "warp pipeline does not fit in shared memory");
+			return SPMV_ERR_ARG;
+		}
+	}
+	WarpFn kern = pick_warp(h);
+	if (!kern) {
+		set_error(SPMV_ERR_ARG, "no warp kernel for format %d", h.desc.format);
+		return SPMV_ERR_ARG;
+	}
+	SPMV_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) h.smem_bytes));
+	int per_sm = h.desc.ctas_per_sm;
+	if (per_sm <= 0) {
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARP_CTA_THREADS, h.smem_bytes));
+		if (per_sm < 1)
+			per_sm = 1;
+	}
+	h.grid = h.num_sms * per_sm;
+	return SPMV_OK;
+}
+
+// Builds the chunk table over the unit pointer P (CSR row_ptr, V = 1; or slice pointer,
+// V = slice height dividing 32) and the per-warp chunk ranges.
+int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
+{
+	cudaStream_t s = h.stream;
+	h.block_cap = h.desc.block_nnz > 0 ? h.desc.block_nnz : 512;
+	if (V > 1 && h.block_cap < V)
+		h.block_cap = V;
+	h.block_cap = (h.block_cap + 7) & ~7;
+	h.stages = h.desc.stages > 0 ? h.desc.stages : 2;
+	SPMV_TRY(warp_geometry(h));
+	int64_t tiles = ceil_div(U, TILE_UNITS);
+	int64_t nch = 0;
+	if (tiles > 0) {
+		DevBuf counts, offs;
+		SPMV_TRY(counts.alloc(tiles * sizeof(int64_t), s));
+		SPMV_TRY(offs.alloc((tiles + 1) * sizeof(int64_t), s));
+		unsigned g = (unsigned) ceil_div(tiles, 128);
+		warp_chunks_kernel<false><<<g, 128, 0, s>>>(d_P, U, V, h.block_cap, counts.as<int64_t>(), nullptr, nullptr);
+		SPMV_CUDA_TRY(cudaGetLastError());
+		SPMV_TRY(scan_exclusive(counts.as<int64_t>(), offs.as<int64_t>(), tiles, s));
+		SPMV_CUDA_TRY(cudaMemcpyAsync(&nch, offs.as<int64_t>() + tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+		SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+		if (nch > INT32_MAX - 1) {
+			set_error(SPMV_ERR_OVERFLOW, "too many chunks");
+			return SPMV_ERR_OVERFLOW;
+		}
+		SPMV_TRY(h.alloc(&h.d_chunks, nch));
+		warp_chunks_kernel<true><<<g, 128, 0, s>>>(d_P, U, V, h.block_cap, nullptr, offs.as<int64_t>(), h.d_chunks);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	h.num_chunks = nch;
+	int64_t W = (int64_t) h.grid * (WARP_CTA_THREADS / 32);
+	h.num_warps = W;
+	SPMV_TRY(h.alloc(&h.d_warp_begin, W + 1));
+	if (nch == 0) {
+		SPMV_CUDA_TRY(cudaMemsetAsync(h.d_warp_begin, 0, (W + 1) * sizeof(int32_t), s));
+		return SPMV_OK;
+	}
+	DevBuf wgt, pre;
+	SPMV_TRY(wgt.alloc(nch * sizeof(int64_t), s));
+	SPMV_TRY(pre.alloc((nch + 1) * sizeof(int64_t), s));
+	chunk_weights_kernel<<<(unsigned) ceil_div(nch, 256), 256, 0, s>>>(h.d_chunks, nch, V, wgt.as<int64_t>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	SPMV_TRY(scan_exclusive(wgt.as<int64_t>(), pre.as<int64_t>(), nch, s));
+	warp_ranges_kernel<<<(unsigned) ceil_div(W + 1, 256), 256, 0, s>>>(h.d_chunks, pre.as<int64_t>(), nch, W,
+			h.d_warp_begin);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	return SPMV_OK;
+}
+
+int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
+{
+	if (h.num_chunks == 0)
+		return SPMV_OK;
+	const int fmt = h.desc.format;
+	WarpArgs a{};
+	a.chunks = h.d_chunks;
+	a.warp_begin = h.d_warp_begin;
+	a.nwarps = h.num_warps;
+	a.x = d_x;
+	a.y = d_y;
+	a.m = h.m;
+	a.cap_al = h.block_cap + 8;
+	a.stages = h.stages;
+	a.stage_bytes = (int) (ceil_div((int64_t) a.cap_al * 12, 128) * 128);
+	a.warp_bytes = h.warp_bytes;
+	a.xbuf_bytes = (fmt == SPMV_FMT_CSR_NAIVE) ? 0 : a.cap_al * 8;
+	a.err = h.d_err;
+	if (fmt == SPMV_FMT_CSR_NAIVE || fmt == SPMV_FMT_CSR_VEC) {
+		a.ptr = h.d_rp;
+		a.cols = h.d_ci;
+		a.vals = h.d_v;
+		a.V = 1;
+	} else if (fmt == SPMV_FMT_SELL_C_S) {
+		a.ptr = h.d_sptr32;
+		a.cols = h.d_scols;
+		a.vals = h.d_svals;
+		a.V = h.desc.sellcs_c;
+		a.ymap = h.d_order;
+	} else {
+		a.ptr = h.d_rcp;
+		a.cols = h.d_ja;
+		a.vals = h.d_a;
+		a.V = h.desc.vec_len;
+		a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
+	}
+	WarpFn kern = pick_warp(h);
+	kern<<<h.grid, WARP_CTA_THREADS, h.smem_bytes, s>>>(a);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	return SPMV_OK;
+}
+
+}  // namespace spmv
