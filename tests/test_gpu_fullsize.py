@@ -93,3 +93,25 @@ def test_other_formats_config2_properties(sb, orc, fmt):
         a = mf.export("a")
         assert np.count_nonzero(a) == np.count_nonzero(v)
         assert np.isclose(np.sum(np.abs(a)), np.sum(np.abs(v)), rtol=1e-12)
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_div_rf_fullsize(sb, orc, cfg):
+    """Config 1: packet bytes identical to the restatement (itself pinned on the reference
+    at this size); config 2: decode round trip of every packet and y within tolerance."""
+    rp, ci, v, x = matrix(sb, cfg)
+    mf = sb.csr_to_format(rp, ci, v, format="div_rf")
+    data = mf.export("div_data")
+    if cfg == "config1":
+        d = orc.div_convert(rp, ci, v, mf.n, T, V, 16384, 0.0)
+        assert np.array_equal(data, d["data"])
+        assert np.array_equal(mf.export("div_groups"), d["group_pos"])
+    else:
+        r, c, val = orc.div_decode_coo(data, V, mf.nnz)
+        order = np.lexsort((c, r))
+        assert np.array_equal(r[order], np.repeat(np.arange(mf.m, dtype=np.int32), np.diff(rp)))
+        assert np.array_equal(c[order], ci)
+        assert np.array_equal(val[order].view(np.uint64), v.view(np.uint64))
+    y = mf.spmv(x)
+    gold, absy = orc.csr_gold(rp, ci, v, x)
+    assert rel_row_error(y, gold, absy) <= TOL

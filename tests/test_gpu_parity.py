@@ -157,7 +157,7 @@ def _rand_csr(m, n, seed, empty_frac=0.2, maxlen=9):
 
 
 @pytest.mark.parametrize("m,n", [(1, 1), (5, 3), (3, 5), (7, 1000), (1001, 17)])
-@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s"])
+@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s", "div_rf"])
 def test_small_and_rectangular(sb, orc, fmt, m, n):
     rp, ci, v = _rand_csr(m, n, m * 31 + n)
     x = np.random.default_rng(1).uniform(-1, 1, n)
@@ -171,12 +171,18 @@ def test_small_and_rectangular(sb, orc, fmt, m, n):
         ref = orc.sell_spmv(orc.sell_convert(rp, ci, v, V, T), m, V, x)
     elif fmt == "sell_sorted":
         ref = orc.sell_sorted_spmv(orc.sell_sorted_convert(rp, ci, v, V, T), m, V, x)
-    else:
+    elif fmt == "sell_c_s":
         ref = orc.sellcs_spmv(orc.sellcs_convert(rp, ci, v, 32, 512), m, 32, x)
+    else:
+        d = orc.div_convert(rp, ci, v, n, T, V, 16384, 0.0)
+        assert np.array_equal(mf.export("div_data"), d["data"])
+        gold, absy = orc.csr_gold(rp, ci, v, x)
+        assert rel_row_error(y, gold, absy) <= TOL
+        return
     assert _eq_bits(y, ref).size == 0
 
 
-@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s"])
+@pytest.mark.parametrize("fmt", REF_FORMATS + ["sell_c_s", "div_rf"])
 def test_all_rows_empty_and_no_entries(sb, fmt):
     m, n = 50, 40
     rp = np.zeros(m + 1, np.int32)
@@ -194,3 +200,61 @@ def test_malformed_csr_is_rejected(sb):
     with pytest.raises(sb.SpmvError) as e:
         sb.csr_to_format(rp, np.array([0, 9], np.int32), np.ones(2), 2, 3, 2)
     assert e.value.status == 2
+
+
+# ------------------------------------------------------------------ DIV-RF
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("pv,pre", [(16384, "div"), (1000, "div1000")])
+def test_div_rf_matches_reference(sb, orc, name, pv, pre):
+    """Packet bytes, packet-group offsets and thread ranges bit-identical to the reference's
+    DIVArray; y within the tolerance of the reference's csr_naive y."""
+    g = load_golden(name)
+    mf = _mk(sb, g, "div_rf", num_threads=T, vec_len=V, div_packet_vals=pv)
+    assert_golden_array(g, f"{pre}_data", mf.export("div_data"))
+    assert_golden_array(g, f"{pre}_group_pos", mf.export("div_groups"))
+    assert_golden_array(g, "div_ranges", mf.export("ranges"))
+    if pre == "div":
+        assert mf.mem_footprint == float(g["mem_div_rf"])
+    y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+    gold, absy = orc.csr_gold(g["row_ptr"], g["col_ind"], g["values"], g["x"])
+    assert rel_row_error(y, g["y_csr_naive"], absy) <= TOL
+    ref_y = g["y_div_rf" if pre == "div" else "y_div_rf_1000"]
+    assert rel_row_error(y, ref_y, absy) <= TOL
+
+
+@pytest.mark.parametrize("name", ["gen_gamma_skew_2000", "dup_values_700", "long_dup_row_40", "empty_rows_333"])
+@pytest.mark.parametrize("L,pv,threads", [(32, 2048, 8), (32, 512, 1), (8, 777, 5), (1, 100, 3)])
+def test_div_rf_other_lane_counts(sb, orc, name, L, pv, threads):
+    """GPU-native settings (32 lanes, smaller packets): bytes equal the restatement's and
+    decode back to the input matrix (the reference's self-check, div.cpp:515-603)."""
+    g = load_golden(name)
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=L, div_packet_vals=pv)
+    data = mf.export("div_data")
+    d = orc.div_convert(rp, ci, v, int(g["n"]), threads, L, pv, 0.0)
+    assert np.array_equal(data, d["data"])
+    assert np.array_equal(mf.export("div_groups"), d["group_pos"])
+    nnz = int(rp[-1])
+    r, c, val = orc.div_decode_coo(data, L, nnz)
+    order = np.lexsort((c, r))
+    assert np.array_equal(r[order], np.repeat(np.arange(rp.size - 1), np.diff(rp)))
+    assert np.array_equal(c[order], ci)
+    assert np.array_equal(val[order].view(np.uint64), v.view(np.uint64))
+    y = mf.spmv(x, np.full(mf.m, 1.0))
+    gold, absy = orc.csr_gold(rp, ci, v, x)
+    assert rel_row_error(y, gold, absy) <= TOL
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-3])
+def test_div_rf_lossy_values(sb, orc, tol):
+    """DIV_VC_TOLERANCE: rounded values, same bytes as the restatement, relative value
+    error within the tolerance."""
+    g = load_golden("gen_diag_1500")
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf = _mk(sb, g, "div_rf", div_tolerance=tol)
+    d = orc.div_convert(rp, ci, v, int(g["n"]), T, V, 16384, tol)
+    assert np.array_equal(mf.export("div_data"), d["data"])
+    r, c, val = orc.div_decode_coo(d["data"], V, int(rp[-1]))
+    order = np.lexsort((c, r))
+    rel = np.abs(val[order] - v) / np.maximum(np.abs(v), 1e-300)
+    assert rel.max() <= tol
