@@ -258,6 +258,8 @@ def run_ours(args):
 
     if head is None:
         raise SystemExit(f"format {args.format} failed: {per_format.get(args.format)}")
+    if args.all_formats:
+        per_format["csr_f32_dot2"] = fp32_variant(sb, torch, dev, rp, ci, v, x, args, per_format)
 
     # e2e: public API with pinned host buffers; x H2D and y D2H inside every step
     mf = head["mf"]
@@ -314,6 +316,38 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def fp32_variant(sb, torch, dev, rp, ci, v, x, args, per_format):
+    """Config 3: FP32 values (rounded once), exact int32 indices, FP32 x/y, Dot2-compensated
+    rows.  Bytes: 8 nnz + 4 (m+1) + 4 n + 4 m.  Error against the FP64 csr_naive result
+    (bit-identical to the reference's), relative to max(|y|, sum |a x|) and plain |dy|/|y|."""
+    m, n, nnz = rp.size - 1, rp.size - 1, int(rp[-1])
+    B32 = nnz * 8 + (m + 1) * 4 + n * 4 + m * 4
+    mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format="csr_naive", values="f32")
+    xd = torch.from_numpy(x.astype(np.float32)).to(dev)
+    yd = torch.empty(m, dtype=torch.float32, device=dev)
+    _, per = time_device(mf, xd, yd, args.steps, args.warmup, torch)
+    med = statistics.median(per)
+    # FP64 reference and sum |a_ij x_j| on the GPU (csr_naive handles)
+    m64 = sb.csr_to_format(rp, ci, v, m, n, nnz, format="csr_naive")
+    y64 = torch.empty(m, dtype=torch.float64, device=dev)
+    m64.spmv(torch.from_numpy(x).to(dev), y64)
+    mabs = sb.csr_to_format(rp, ci, np.abs(v), m, n, nnz, format="csr_naive")
+    absy = torch.empty(m, dtype=torch.float64, device=dev)
+    mabs.spmv(torch.from_numpy(np.abs(x)).to(dev), absy)
+    torch.cuda.synchronize()
+    d = (yd.double() - y64).abs()
+    cond = (d / torch.maximum(y64.abs(), absy).clamp_min(1e-300)).cpu().numpy()
+    nz = y64.abs() > 0
+    plain = (d[nz] / y64.abs()[nz]).cpu().numpy()
+    t64 = per_format.get("csr_naive", {}).get("ms_median")
+    return {"ms_median": med, "gbs": B32 * 1e-9 / (med * 1e-3), "gflops": 2.0 * nnz * 1e-9 / (med * 1e-3),
+            "bytes_per_spmv": B32, "speedup_vs_fp64_csr": (t64 / med) if t64 else None,
+            "max_rel_err_cond": float(cond.max()), "mean_rel_err_cond": float(cond.mean()),
+            "max_rel_err_plain": float(plain.max()) if plain.size else 0.0,
+            "mean_rel_err_plain": float(plain.mean()) if plain.size else 0.0,
+            "convert_ms": mf.convert_ms}
 
 
 def cpu_baseline(fmt, rp, ci, v, x, B, sample_s=10.0):

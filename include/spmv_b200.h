@@ -142,8 +142,11 @@ int spmv_run(spmv_handle * h, const double * x, double * y);
  * are reported by the next spmv_sync() / spmv_run(). */
 int spmv_run_device(spmv_handle * h, const double * d_x, double * d_y, void * stream);
 
-/* FP32 variant entry: float x / y (values stored FP32, handle created with values = F32). */
+/* FP32 variant (handle created with values = SPMV_VALUES_F32): float x / y, device-resident
+ * or host buffers (the reference's `_f` executables, ValueType = float, make.sh:148).
+ * spmv_run() also accepts an FP32 handle: x is rounded to FP32 once and y widened. */
 int spmv_run_device_f32(spmv_handle * h, const float * d_x, float * d_y, void * stream);
+int spmv_run_f32(spmv_handle * h, const float * x, float * y);
 
 /* Waits for the handle's stream and returns the first device-side error, if any. */
 int spmv_sync(spmv_handle * h);

@@ -40,6 +40,7 @@ def lib():
             "orc_csr_spmv": (None, [P, P, P, c_long, P, P]),
             "orc_csr_vec_spmv": (None, [P, P, P, c_long, c_long, P, P]),
             "orc_csr_gold": (None, [P, P, P, c_long, P, P, P]),
+            "orc_csr_f32_dot2": (None, [P, P, P, c_long, P, P]),
             "orc_sell_size": (c_long, [P, c_long, c_long]),
             "orc_sell_convert": (None, [P, P, P, c_long, c_long, c_long, P, P, P, P]),
             "orc_sell_spmv": (None, [P, P, P, c_long, c_long, P, P]),
@@ -94,6 +95,16 @@ def csr_vec_spmv(rp, ci, v, x, L=4):
     m = rp.size - 1
     y = np.empty(m, np.float64)
     lib().orc_csr_vec_spmv(_p(rp), _p(ci), _p(v), m, L, _p(x), _p(y))
+    return y
+
+
+def csr_f32_dot2(rp, ci, v32, x32):
+    """FP32 values / x, Dot2-compensated FP32 row sums."""
+    rp, ci = _c(rp, np.int32), _c(ci, np.int32)
+    v32, x32 = _c(v32, np.float32), _c(x32, np.float32)
+    m = rp.size - 1
+    y = np.empty(m, np.float32)
+    lib().orc_csr_f32_dot2(_p(rp), _p(ci), _p(v32), m, _p(x32), _p(y))
     return y
 
 

@@ -157,6 +157,29 @@ void orc_csr_gold(const int32_t * rp, const int32_t * ci, const double * v, long
 	}
 }
 
+/* FP32 variant: values and x rounded to FP32, each row summed with the compensated dot
+ * product Dot2 (Ogita, Rump, Oishi, SIAM J. Sci. Comput. 26(6), 2005): TwoProduct by
+ * fmaf, Knuth's TwoSum, errors accumulated in a second FP32 sum; y = s + c.  The GPU's
+ * FP32 kernel sums rows in the same sequential order. */
+void orc_csr_f32_dot2(const int32_t * rp, const int32_t * ci, const float * v, long m, const float * x, float * y)
+{
+	#pragma omp parallel for schedule(static)
+	for (long i = 0; i < m; i++) {
+		float s = 0.0f, c = 0.0f;
+		for (long j = rp[i]; j < rp[i + 1]; j++) {
+			float a = v[j], b = x[ci[j]];
+			float p = a * b;
+			float pe = fmaf(a, b, -p);
+			float t = s + p;
+			float z = t - s;
+			float e = (s - (t - z)) + (p - z);
+			s = t;
+			c = c + (e + pe);
+		}
+		y[i] = s + c;
+	}
+}
+
 /* ======================================================================================
  * SELL (slice height V, column-major slices)
  * ====================================================================================== */

@@ -30,6 +30,9 @@ void orc_csr_vec_spmv(const int32_t * rp, const int32_t * ci, const double * v, 
  * after src/bench_spmv.cpp:150-172 (which uses _Float128). Also returns sum_j |a_ij x_j|. */
 void orc_csr_gold(const int32_t * rp, const int32_t * ci, const double * v, long m, const double * x, double * y, double * absy);
 
+/* FP32 storage variant: compensated (Dot2) FP32 row sums. */
+void orc_csr_f32_dot2(const int32_t * rp, const int32_t * ci, const float * v, long m, const float * x, float * y);
+
 /* ---- SELL (src/spmv_kernels/sell.cpp) ---- */
 long orc_sell_size(const int32_t * rp, long m, long V);
 void orc_sell_convert(const int32_t * rp, const int32_t * ci, const double * v, long m, long V, long T,

@@ -156,6 +156,16 @@ class Matrix_Format:
             if st:
                 _raise(st)
             return y
+        if getattr(x, "dtype", None) == np.float32 and getattr(self, "_f32", False):
+            xf = _host(x, np.float32)
+            if y is None:
+                y = np.empty(self.m, np.float32)
+            if xf.size < self.n or not (isinstance(y, np.ndarray) and y.dtype == np.float32 and y.size >= self.m):
+                raise ValueError("x / y must be float32 arrays of n / m elements")
+            st = lib.spmv_run_f32(self._h, xf.ctypes.data, y.ctypes.data)
+            if st:
+                _raise(st)
+            return y
         xh = _host(x, np.float64)
         if xh.size < self.n:
             raise ValueError(f"x needs {self.n} elements")

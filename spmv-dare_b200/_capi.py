@@ -74,6 +74,7 @@ SIGNATURES = {
     "spmv_run": (c_int, [c_void_p, c_void_p, c_void_p]),
     "spmv_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_run_device_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_run_f32": (c_int, [c_void_p, c_void_p, c_void_p]),
     "spmv_sync": (c_int, [c_void_p]),
     "spmv_get_info": (c_int, [c_void_p, POINTER(Info)]),
     "spmv_export": (c_int, [c_void_p, c_int32, c_void_p, POINTER(c_int64)]),

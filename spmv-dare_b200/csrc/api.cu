@@ -156,6 +156,10 @@ static int convert_all(Handle & h)
 	switch (h.desc.format) {
 	case SPMV_FMT_CSR_NAIVE:
 	case SPMV_FMT_CSR_VEC:
+		if (h.desc.values == SPMV_VALUES_F32) {
+			SPMV_TRY(convert_f32(h));
+			break;
+		}
 		SPMV_TRY(convert_csr(h));
 		h.kernels_per_run = (h.num_blocks > 0 || h.num_chunks > 0) ? 1 : 0;
 		break;
@@ -175,6 +179,8 @@ static int convert_all(Handle & h)
 	SPMV_CUDA_TRY(cudaStreamSynchronize(h.stream));
 	set_footprints(h);
 	h.name = kNames[h.desc.format];
+	if (h.desc.values == SPMV_VALUES_F32)
+		h.name = "Naive_CSR_F32_Dot2_B200";
 	return SPMV_OK;
 }
 
@@ -361,10 +367,6 @@ int spmv_run(spmv_handle * H, const double * x, double * y)
 		return SPMV_ERR_ARG;
 	}
 	Handle & h = H->h;
-	if (h.desc.values != SPMV_VALUES_F64) {
-		spmv::set_error(SPMV_ERR_ARG, "handle stores FP32 values: use spmv_run_device_f32");
-		return SPMV_ERR_ARG;
-	}
 	if (!h.d_x) {
 		SPMV_TRY(h.alloc(&h.d_x, h.n + 1));
 		SPMV_TRY(h.alloc(&h.d_y, h.m + 1));
@@ -372,9 +374,45 @@ int spmv_run(spmv_handle * H, const double * x, double * y)
 	cudaStream_t s = h.stream;
 	if (h.n > 0)
 		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_x, x, h.n * sizeof(double), cudaMemcpyHostToDevice, s));
-	SPMV_TRY(spmv::launch_spmv(h, h.d_x, h.d_y, s));
+	if (h.desc.values == SPMV_VALUES_F32) {
+		// FP32 handle driven with FP64 buffers: round x once, widen y
+		if (!h.d_xf) {
+			SPMV_TRY(h.alloc(&h.d_xf, h.n + 1));
+			SPMV_TRY(h.alloc(&h.d_yf, h.m + 1));
+		}
+		SPMV_TRY(spmv::convert_vector_d2f(h.d_x, h.d_xf, h.n, s));
+		SPMV_TRY(spmv::launch_spmv_f32(h, h.d_xf, h.d_yf, s));
+		SPMV_TRY(spmv::convert_vector_f2d(h.d_yf, h.d_y, h.m, s));
+	} else {
+		SPMV_TRY(spmv::launch_spmv(h, h.d_x, h.d_y, s));
+	}
 	if (h.m > 0)
 		SPMV_CUDA_TRY(cudaMemcpyAsync(y, h.d_y, h.m * sizeof(double), cudaMemcpyDeviceToHost, s));
+	return spmv::check_device_error(h);
+}
+
+int spmv_run_f32(spmv_handle * H, const float * x, float * y)
+{
+	spmv::clear_error();
+	if (!H || (!x && H->h.n > 0) || (!y && H->h.m > 0)) {
+		spmv::set_error(SPMV_ERR_ARG, "null handle or vector");
+		return SPMV_ERR_ARG;
+	}
+	Handle & h = H->h;
+	if (h.desc.values != SPMV_VALUES_F32) {
+		spmv::set_error(SPMV_ERR_ARG, "handle stores FP64 values: use spmv_run");
+		return SPMV_ERR_ARG;
+	}
+	if (!h.d_xf) {
+		SPMV_TRY(h.alloc(&h.d_xf, h.n + 1));
+		SPMV_TRY(h.alloc(&h.d_yf, h.m + 1));
+	}
+	cudaStream_t s = h.stream;
+	if (h.n > 0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_xf, x, h.n * sizeof(float), cudaMemcpyHostToDevice, s));
+	SPMV_TRY(spmv::launch_spmv_f32(h, h.d_xf, h.d_yf, s));
+	if (h.m > 0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(y, h.d_yf, h.m * sizeof(float), cudaMemcpyDeviceToHost, s));
 	return spmv::check_device_error(h);
 }
 

@@ -104,6 +104,8 @@ struct Handle {
 	// host-buffer path staging
 	double * d_x = nullptr;
 	double * d_y = nullptr;
+	float * d_xf = nullptr;
+	float * d_yf = nullptr;
 
 	std::vector<void *> allocations;    // everything above, freed by destroy
 	double mem_footprint = 0;
@@ -135,6 +137,9 @@ int convert_csr(Handle & h);
 int convert_sell(Handle & h, bool sorted);
 int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
+int convert_f32(Handle & h);
+int convert_vector_d2f(const double * in, float * out, int64_t n, cudaStream_t s);
+int convert_vector_f2d(const float * in, double * out, int64_t n, cudaStream_t s);
 
 
 // Builds the execution schedule of the chosen kernel over the unit pointer P (CSR row_ptr

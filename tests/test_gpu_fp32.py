@@ -1,0 +1,50 @@
+"""FP32 storage variant (FP32 values, exact int32 indices, Dot2-compensated FP32 rows).
+
+Bars: y bit-identical to the oracle's sequential Dot2 rows (rows that fit one staged
+block; longer rows use a compensated tree and are checked by tolerance), and max relative
+error against the FP64 result <= 1e-6 per row, relative to max(|y_i|, sum_j |a_ij x_j|).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, rel_row_error
+
+pytestmark = pytest.mark.gpu
+
+TOL_F32 = 1e-6
+
+
+def _run(sb, rp, ci, v, x, **kw):
+    mf = sb.csr_to_format(rp, ci, v, rp.size - 1, x.size, int(rp[-1]), format="csr_naive", values="f32", **kw)
+    y32 = mf.spmv(x.astype(np.float32), np.full(mf.m, 1.0, np.float32))
+    y64 = mf.spmv(x, np.full(mf.m, 1.0))          # FP64 buffers: x rounded once, y widened
+    return mf, y32, y64
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fp32_variant_matches_dot2_oracle(sb, orc, name):
+    g = load_golden(name)
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf, y32, y64 = _run(sb, rp, ci, v, x)
+    assert mf.export("values").dtype == np.float32
+    assert np.array_equal(mf.export("values"), v.astype(np.float32))
+    ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
+    lens = np.diff(rp)
+    short = lens <= 2048
+    assert np.array_equal(y32[short].view(np.uint32), ref[short].view(np.uint32))
+    assert np.array_equal(y64.astype(np.float32).view(np.uint32), y32.view(np.uint32))
+    gold, absy = orc.csr_gold(rp, ci, v, x)
+    assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
+
+
+def test_fp32_device_path(sb, orc):
+    import torch
+
+    g = load_golden("gen_gamma_skew_2000")
+    rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+    mf, y32, _ = _run(sb, rp, ci, v, x)
+    xd = torch.from_numpy(x.astype(np.float32)).cuda()
+    yd = torch.zeros(mf.m, dtype=torch.float32, device="cuda")
+    mf.spmv(xd, yd)
+    torch.cuda.synchronize()
+    assert np.array_equal(yd.cpu().numpy().view(np.uint32), y32.view(np.uint32))
