@@ -304,7 +304,7 @@ def run_ours(args):
                      else "fallback 6.65 TB/s"},
         "gpu_launches": args.steps * mf.kernels_per_run,
         "clocks": head["clocks"],
-        "per_format": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in r.items()}
+        "per_format": {k: {kk: (float(f"{vv:.5g}") if isinstance(vv, float) else vv) for kk, vv in r.items()}
                        for k, r in per_format.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -324,7 +324,7 @@ def fp32_variant(sb, torch, dev, rp, ci, v, x, args, per_format):
     (bit-identical to the reference's), relative to max(|y|, sum |a x|) and plain |dy|/|y|."""
     m, n, nnz = rp.size - 1, rp.size - 1, int(rp[-1])
     B32 = nnz * 8 + (m + 1) * 4 + n * 4 + m * 4
-    mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format="csr_naive", values="f32")
+    mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format="csr_naive", value_type="f32")
     xd = torch.from_numpy(x.astype(np.float32)).to(dev)
     yd = torch.empty(m, dtype=torch.float32, device=dev)
     _, per = time_device(mf, xd, yd, args.steps, args.warmup, torch)

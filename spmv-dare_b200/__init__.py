@@ -69,7 +69,8 @@ def _desc(format, params):
     for k, v in params.items():
         if v is None:
             continue
-        if k == "values":
+        if k == "value_type":           # the descriptor's `values` field
+            k = "values"
             v = {"f64": VALUES_F64, "f32": VALUES_F32}.get(v, v)
         if not hasattr(d, k) or k in ("format", "reserved"):
             raise TypeError(f"unknown format parameter {k!r}")
@@ -228,7 +229,8 @@ def csr_to_format(row_ptr, col_ind, values, m=None, n=None, nnz=None, symmetric=
     Inputs may be host arrays (copied, as every reference format deep-copies) or CUDA torch
     tensors (converted device-to-device).  `params` are spmv_format_desc fields
     (num_threads, vec_len, sellcs_c, sellcs_sigma, div_packet_vals, div_tolerance, exact,
-    values, block_nnz, block_rows, stages, ctas_per_sm)."""
+    block_nnz, block_rows, stages, ctas_per_sm, threads, kernel) and value_type ("f64", or
+    "f32" for the FP32 storage variant)."""
     desc = _desc(format, params)
     st = c_int(0)
     lib = library()

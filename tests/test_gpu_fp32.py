@@ -15,7 +15,7 @@ TOL_F32 = 1e-6
 
 
 def _run(sb, rp, ci, v, x, **kw):
-    mf = sb.csr_to_format(rp, ci, v, rp.size - 1, x.size, int(rp[-1]), format="csr_naive", values="f32", **kw)
+    mf = sb.csr_to_format(rp, ci, v, rp.size - 1, x.size, int(rp[-1]), format="csr_naive", value_type="f32", **kw)
     y32 = mf.spmv(x.astype(np.float32), np.full(mf.m, 1.0, np.float32))
     y64 = mf.spmv(x, np.full(mf.m, 1.0))          # FP64 buffers: x rounded once, y widened
     return mf, y32, y64
