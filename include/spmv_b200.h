@@ -189,6 +189,29 @@ const char * spmv_last_error(void);
 int spmv_statistics_print_labels(char * buf, int64_t buf_n);
 int spmv_statistics_print_data(const spmv_handle * h, char * buf, int64_t buf_n);
 
+/* ---------------------------------------------------------------- batched SpMV */
+/*
+ * Many matrices, one persistent launch.  Each matrix is converted with its own descriptor
+ * (an autotuner's pick: csr_naive, sell, sell_sorted or sell_c_s with its slice
+ * parameters; the staging geometry -- block_nnz, stages, threads, exact -- of descs[0]
+ * applies to the whole batch).  The staged blocks of all matrices form one work queue that
+ * the kernel's CTAs drain through an atomic counter.  x and y are the matrices' vectors
+ * concatenated in order (offsets from spmv_batch_info).  No reference counterpart: the
+ * reference runs one matrix per process (src/bench.cpp:470-663).
+ */
+typedef struct spmv_batch spmv_batch;
+spmv_batch * spmv_batch_create(int32_t count, const int32_t * const * row_ptrs, const int32_t * const * col_inds,
+		const double * const * values, const int64_t * ms, const int64_t * ns, const spmv_format_desc * descs,
+		int * status);
+/* One launch (work-queue reset + persistent kernel) on `stream` (NULL: the batch's stream). */
+int spmv_batch_run_device(spmv_batch * b, const double * d_x, double * d_y, void * stream);
+/* The same two operations captured once into a CUDA graph (per (d_x, d_y) pair) and replayed. */
+int spmv_batch_run_graph(spmv_batch * b, const double * d_x, double * d_y, void * stream);
+int spmv_batch_sync(spmv_batch * b);
+int spmv_batch_info(const spmv_batch * b, int64_t * total_x, int64_t * total_y, int64_t * total_nnz,
+		int64_t * x_offsets, int64_t * y_offsets, int64_t * num_blocks);
+void spmv_batch_destroy(spmv_batch * b);
+
 /* ---------------------------------------------------------------- artificial matrices */
 /*
  * The reference's artificial matrix generator, restated natively on the host

@@ -29,7 +29,7 @@ from ._capi import FORMATS, VALUES_F32, VALUES_F64
 
 __all__ = [
     "SpmvError", "Matrix_Format", "csr_to_format", "statistics_print_labels", "generate_artificial",
-    "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version",
+    "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version", "Batch",
 ]
 
 
@@ -265,6 +265,77 @@ def csr_to_format(row_ptr, col_ind, values, m=None, n=None, nnz=None, symmetric=
     mf = Matrix_Format(h, format)
     mf._f32 = desc.values == VALUES_F32
     return mf
+
+
+class Batch:
+    """Many matrices in one persistent launch (spmv_batch_* of the C ABI).
+
+    matrices: list of (row_ptr, col_ind, values, m, n); formats: one format name (or
+    dict of descriptor fields incl. "format") per matrix; geometry: block_nnz, stages,
+    threads, exact for the whole batch.  x / y are the matrices' vectors concatenated
+    (see x_offsets / y_offsets)."""
+
+    def __init__(self, matrices, formats, **geometry):
+        lib = library()
+        cnt = len(matrices)
+        if len(formats) != cnt:
+            raise ValueError("one format per matrix")
+        descs = (_capi.FormatDesc * max(cnt, 1))()
+        self._keep = []
+        rps = (ctypes.c_void_p * max(cnt, 1))()
+        cis = (ctypes.c_void_p * max(cnt, 1))()
+        vvs = (ctypes.c_void_p * max(cnt, 1))()
+        ms = np.empty(max(cnt, 1), np.int64)
+        ns = np.empty(max(cnt, 1), np.int64)
+        for i, ((rp, ci, vv, m, n), f) in enumerate(zip(matrices, formats)):
+            params = dict(f) if isinstance(f, dict) else {"format": f}
+            fmt = params.pop("format")
+            params.update(geometry)
+            descs[i] = _desc(fmt, params)
+            rp, ci, vv = _host(rp, np.int32), _host(ci, np.int32), _host(vv, np.float64)
+            self._keep += [rp, ci, vv]
+            rps[i], cis[i], vvs[i] = rp.ctypes.data, ci.ctypes.data if ci.size else None, vv.ctypes.data if vv.size else None
+            ms[i], ns[i] = m, n
+        st = c_int(0)
+        self._b = lib.spmv_batch_create(cnt, ctypes.cast(rps, ctypes.c_void_p), ctypes.cast(cis, ctypes.c_void_p),
+                                        ctypes.cast(vvs, ctypes.c_void_p), ms.ctypes.data, ns.ctypes.data,
+                                        ctypes.cast(descs, ctypes.c_void_p), byref(st))
+        self._keep = None
+        if not self._b:
+            _raise(st.value)
+        tx, ty, tn, nb = c_int64(), c_int64(), c_int64(), c_int64()
+        self.x_offsets = np.empty(max(cnt, 1), np.int64)
+        self.y_offsets = np.empty(max(cnt, 1), np.int64)
+        lib.spmv_batch_info(self._b, byref(tx), byref(ty), byref(tn), self.x_offsets.ctypes.data,
+                            self.y_offsets.ctypes.data, byref(nb))
+        self.x_offsets, self.y_offsets = self.x_offsets[:cnt], self.y_offsets[:cnt]
+        self.total_x, self.total_y, self.total_nnz, self.num_blocks = tx.value, ty.value, tn.value, nb.value
+        self.count = cnt
+
+    def spmv(self, xd, yd, graph=False, stream=None):
+        """xd, yd: CUDA float64 tensors of total_x / total_y elements."""
+        s = _torch_stream(xd.device, stream)
+        f = library().spmv_batch_run_graph if graph else library().spmv_batch_run_device
+        st = f(self._b, xd.data_ptr(), yd.data_ptr(), s)
+        if st:
+            _raise(st)
+        return yd
+
+    def sync(self):
+        st = library().spmv_batch_sync(self._b)
+        if st:
+            _raise(st)
+
+    def destroy(self):
+        if getattr(self, "_b", None):
+            library().spmv_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def statistics_print_labels():

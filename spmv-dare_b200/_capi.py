@@ -88,6 +88,13 @@ SIGNATURES = {
     "spmv_artgen_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_artgen_destroy": (None, [c_void_p]),
     "spmv_version": (c_char_p, []),
+    "spmv_batch_create": (c_void_p, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     POINTER(c_int)]),
+    "spmv_batch_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_batch_run_graph": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_batch_sync": (c_int, [c_void_p]),
+    "spmv_batch_info": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_batch_destroy": (None, [c_void_p]),
 }
 
 _lib = None

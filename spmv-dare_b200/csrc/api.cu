@@ -258,6 +258,13 @@ struct spmv_handle {
 	Handle h;
 };
 
+namespace spmv {
+Handle * handle_of(spmv_handle * H)
+{
+	return &H->h;
+}
+}  // namespace spmv
+
 extern "C" {
 
 void spmv_format_desc_init(spmv_format_desc * d, int32_t format)

@@ -32,6 +32,36 @@ struct WarpChunk {
 };
 
 enum class Kind { CSR = 0, SLICED = 1 };
+
+// One matrix of a batch (device table).
+struct BatchMat {
+	int32_t kind;                  // 0: csr_naive order; 1: slices, one FMA per column
+	int32_t V;                     // slice height (kind 1)
+	int64_t m;
+	const int32_t * ptr;           // row_ptr or slice pointer
+	const int32_t * cols;
+	const double * vals;
+	const int32_t * ymap;          // row map of sorted slices, or null
+	int64_t x_off, y_off;          // offsets into the batch's concatenated x and y
+};
+
+struct BatchArgs {
+	const StagedBlock * blocks;
+	const int32_t * bmat;          // matrix of each block
+	int64_t nblocks;
+	const BatchMat * mats;
+	const double * x;
+	double * y;
+	int cap_al;
+	int stages;
+	int stage_bytes;
+	int exact;
+	unsigned long long * counter;  // work-queue head, zero at launch
+	int * err;
+};
+
+int batch_launch(const BatchArgs & b, int grid, int threads, size_t smem, cudaStream_t s);
+int batch_occupancy(int threads, size_t smem, int * per_sm);
 enum class Arith { SEQ_SPLIT = 0, SEQ_FMA = 1, LANES_FMA = 2 };
 
 struct Handle {

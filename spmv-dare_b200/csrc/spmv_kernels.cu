@@ -222,8 +222,92 @@ __device__ __forceinline__ void staged_long_unit(const StagedArgs & a, const Sta
 		if (threadIdx.x < V) {
 			const int64_t row = sl * V + threadIdx.x;
 			if (row < a.m)
-				a.y[YMAP ? a.ymap[row] : row] = acc;
+				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
 		}
+	}
+}
+
+// One staged block (or one long unit) of a staged kernel: gather, then rows in the
+// reference order.  `smem_stage` is the block's stage buffer, `xb` the gather buffer.
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void staged_block(const StagedArgs & a, const StagedBlock & d, uint8_t * smem_stage, double * xb)
+{
+	if (d.units >= 0) {
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		const int off = (int) (d.elem0 - e0);
+		const int cnt = d.elems;
+		double * sv = reinterpret_cast<double *>(smem_stage);
+		const int32_t * sc = reinterpret_cast<const int32_t *>(smem_stage + (size_t) a.cap_al * 8);
+		// row bounds of this thread's first row, loaded before the gather so their
+		// latency overlaps it
+		int js0 = 0, je0 = 0;
+		if (K == Kind::CSR && (int) threadIdx.x < d.units) {
+			const int64_t r = (int64_t) d.unit0 + threadIdx.x;
+			js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+			je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+		}
+		// 1) gather x for every staged entry, all threads, many loads in flight
+		#pragma unroll 4
+		for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+			const double xv = ldg(a.x + sc[off + e]);
+			if (A == Arith::SEQ_SPLIT)
+				sv[off + e] = __dmul_rn(sv[off + e], xv);   // the reference's rounded product
+			else
+				xb[off + e] = xv;
+		}
+		__syncthreads();
+		// 2) one thread per row, reference order, operands in shared memory
+		if (K == Kind::CSR) {
+			for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
+				const int64_t r = (int64_t) d.unit0 + u;
+				const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
+				const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
+				double sum = 0.0;
+				if (A == Arith::SEQ_SPLIT) {
+					#pragma unroll 4
+					for (int j = js; j < je; j++)
+						sum = __dadd_rn(sum, sv[j]);
+				} else if (A == Arith::SEQ_FMA) {
+					#pragma unroll 4
+					for (int j = js; j < je; j++)
+						sum = __fma_rn(sv[j], xb[j], sum);
+				} else {
+					double ln[L];
+					#pragma unroll
+					for (int l = 0; l < L; l++)
+						ln[l] = 0.0;
+					const int jv = js + ((je - js) & ~(L - 1));
+					for (int j = js; j < jv; j += L) {
+						#pragma unroll
+						for (int l = 0; l < L; l++)
+							ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
+					}
+					sum = lanes_reduce<L>(ln);
+					for (int j = jv; j < je; j++)
+						sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
+				}
+				a.y[r] = sum;
+			}
+		} else {
+			const int V = a.V;
+			const int nrow = d.units * V;
+			for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
+				const int64_t sl = (int64_t) d.unit0 + u / V;
+				const int lane = u % V;
+				const int64_t row = sl * V + lane;
+				if (row >= a.m)
+					continue;
+				const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
+				const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+				double acc = 0.0;
+				#pragma unroll 4
+				for (int k = 0; k < w; k++)
+					acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
+				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+			}
+		}
+	} else {
+		staged_long_unit<K, A, L, YMAP>(a, d, xb);
 	}
 }
 
@@ -259,89 +343,98 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 			return;
 		}
-		if (d.units >= 0) {
-			const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
-			const int off = (int) (d.elem0 - e0);
-			const int cnt = d.elems;
-			double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
-			const int32_t * sc = reinterpret_cast<const int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
-			// row bounds of this thread's first row, loaded before the gather so their
-			// latency overlaps it
-			int js0 = 0, je0 = 0;
-			if (K == Kind::CSR && (int) threadIdx.x < d.units) {
-				const int64_t r = (int64_t) d.unit0 + threadIdx.x;
-				js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
-				je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
-			}
-			// 1) gather x for every staged entry, all threads, many loads in flight
-			#pragma unroll 4
-			for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-				const double xv = ldg(a.x + sc[off + e]);
-				if (A == Arith::SEQ_SPLIT)
-					sv[off + e] = __dmul_rn(sv[off + e], xv);   // the reference's rounded product
-				else
-					xb[off + e] = xv;
-			}
-			__syncthreads();
-			// 2) one thread per row, reference order, operands in shared memory
-			if (K == Kind::CSR) {
-				for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
-					const int64_t r = (int64_t) d.unit0 + u;
-					const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
-					const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
-					double sum = 0.0;
-					if (A == Arith::SEQ_SPLIT) {
-						#pragma unroll 4
-						for (int j = js; j < je; j++)
-							sum = __dadd_rn(sum, sv[j]);
-					} else if (A == Arith::SEQ_FMA) {
-						#pragma unroll 4
-						for (int j = js; j < je; j++)
-							sum = __fma_rn(sv[j], xb[j], sum);
-					} else {
-						double ln[L];
-						#pragma unroll
-						for (int l = 0; l < L; l++)
-							ln[l] = 0.0;
-						const int jv = js + ((je - js) & ~(L - 1));
-						for (int j = js; j < jv; j += L) {
-							#pragma unroll
-							for (int l = 0; l < L; l++)
-								ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
-						}
-						sum = lanes_reduce<L>(ln);
-						for (int j = jv; j < je; j++)
-							sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
-					}
-					a.y[r] = sum;
-				}
-			} else {
-				const int V = a.V;
-				const int nrow = d.units * V;
-				for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
-					const int64_t sl = (int64_t) d.unit0 + u / V;
-					const int lane = u % V;
-					const int64_t row = sl * V + lane;
-					if (row >= a.m)
-						continue;
-					const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
-					const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
-					double acc = 0.0;
-					#pragma unroll 4
-					for (int k = 0; k < w; k++)
-						acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
-					a.y[YMAP ? a.ymap[row] : row] = acc;
-				}
-			}
-		} else {
-			staged_long_unit<K, A, L, YMAP>(a, d, xb);
-		}
+		staged_block<K, A, L, YMAP>(a, d, smem + (size_t) s * a.stage_bytes, xb);
 		__syncthreads();
 		if (threadIdx.x == 0) {
 			int64_t nb = b + (int64_t) a.stages * gridDim.x;
 			if (nb < a.nblocks)
 				staged_issue(a, nb, s, smem, bars);
 		}
+	}
+}
+
+// ------------------------------------------------------------------ batched SpMV
+// Many matrices in one persistent launch.  The staged blocks of every matrix form one
+// work queue (long units first); CTAs claim blocks with an atomic counter (dynamic, so
+// uneven matrices balance), prefetch `stages` claims ahead through the bulk-copy ring, and
+// run the block with its matrix's format: kind 0 = csr_naive order, kind 1 = slices with
+// one FMA per column (sell, sell_sorted, sell_c_s).
+__device__ __forceinline__ void batch_issue(const BatchArgs & b, int64_t c, int s, uint8_t * smem, uint64_t * bars,
+		int64_t * claim)
+{
+	claim[s] = c < b.nblocks ? c : -1;
+	if (c >= b.nblocks) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const StagedBlock d = b.blocks[c];
+	if (d.units < 0 || d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const BatchMat mt = b.mats[b.bmat[c]];
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	double * sv = reinterpret_cast<double *>(smem + (size_t) s * b.stage_bytes);
+	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * b.stage_bytes + (size_t) b.cap_al * 8);
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 12u);
+	bulk_g2s(sv, mt.vals + e0, cnt * 8u, &bars[s]);
+	bulk_g2s(sc, mt.cols + e0, cnt * 4u, &bars[s]);
+}
+
+__global__ void __launch_bounds__(STAGED_MAX_THREADS) batch_kernel(BatchArgs b)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	__shared__ int64_t claim[8];
+	double * xb = reinterpret_cast<double *>(smem + (size_t) b.stages * b.stage_bytes);
+	uint64_t * bars = reinterpret_cast<uint64_t *>(smem + (size_t) b.stages * b.stage_bytes + (size_t) b.cap_al * 8);
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < b.stages; s++)
+			mbar_init(&bars[s], 1);
+		mbar_fence_init();
+	}
+	__syncthreads();
+	if (threadIdx.x == 0)
+		for (int s = 0; s < b.stages; s++)
+			batch_issue(b, (int64_t) atomicAdd(b.counter, 1ULL), s, smem, bars, claim);
+	for (int it = 0;; it++) {
+		const int s = it % b.stages;
+		const uint32_t parity = (uint32_t) ((it / b.stages) & 1);
+		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
+		if (__syncthreads_or(!ok)) {
+			if (threadIdx.x == 0)
+				dev_flag_error(b.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		const int64_t c = claim[s];
+		if (c < 0)
+			break;          // the queue is drained; every later slot of this ring is empty too
+		const StagedBlock d = b.blocks[c];
+		const BatchMat mt = b.mats[b.bmat[c]];
+		StagedArgs a{};
+		a.ptr = mt.ptr;
+		a.cols = mt.cols;
+		a.vals = mt.vals;
+		a.ymap = mt.ymap;
+		a.x = b.x + mt.x_off;
+		a.y = b.y + mt.y_off;
+		a.m = mt.m;
+		a.V = mt.V;
+		a.cap_al = b.cap_al;
+		a.stages = b.stages;
+		a.stage_bytes = b.stage_bytes;
+		a.exact = b.exact;
+		a.err = b.err;
+		uint8_t * stage = smem + (size_t) s * b.stage_bytes;
+		if (mt.kind == 0)
+			staged_block<Kind::CSR, Arith::SEQ_SPLIT, 1, false>(a, d, stage, xb);
+		else
+			staged_block<Kind::SLICED, Arith::SEQ_FMA, 1, true>(a, d, stage, xb);
+		__syncthreads();
+		if (threadIdx.x == 0)
+			batch_issue(b, (int64_t) atomicAdd(b.counter, 1ULL), s, smem, bars, claim);
 	}
 }
 
@@ -398,7 +491,7 @@ __global__ void __launch_bounds__(256) sliced_kernel(SlicedArgs a)
 			const int64_t o = (int64_t) k * C;
 			acc = __fma_rn(v[o], ldg(a.x + c[o]), acc);
 		}
-		a.y[YMAP ? a.ymap[row] : row] = acc;
+		a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
 	}
 }
 
@@ -428,6 +521,25 @@ StagedFn pick_staged(const Handle & h)
 }
 
 }  // namespace
+
+int batch_launch(const BatchArgs & b, int grid, int threads, size_t smem, cudaStream_t s)
+{
+	static bool configured = false;
+	if (!configured) {
+		SPMV_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+		configured = true;
+	}
+	batch_kernel<<<grid, threads, smem, s>>>(b);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	return SPMV_OK;
+}
+
+int batch_occupancy(int threads, size_t smem, int * per_sm)
+{
+	SPMV_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+	SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, batch_kernel, threads, smem));
+	return SPMV_OK;
+}
 
 // Grid / shared-memory geometry of the staged kernel for this handle.
 int staged_geometry(Handle & h)
