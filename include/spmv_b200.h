@@ -148,6 +148,29 @@ int spmv_run_device(spmv_handle * h, const double * d_x, double * d_y, void * st
 int spmv_run_device_f32(spmv_handle * h, const float * d_x, float * d_y, void * stream);
 int spmv_run_f32(spmv_handle * h, const float * x, float * y);
 
+/*
+ * Allocation-free FP32-storage SpMV with FP64 vectors on the device.  No counterpart in
+ * the reference.  For callers that must not allocate device memory during a run: code
+ * whose device memory comes from a fixed pool or an arena it does not own, or a call made
+ * while a stream is being captured into a CUDA graph, where cudaMalloc is not allowed.
+ * Does what spmv_run() does with an FP32 handle and FP64 buffers (x rounded to FP32 once,
+ * the Dot2-compensated FP32 SpMV, y widened to FP64), but on device vectors, enqueued on
+ * `stream` (NULL: the handle's stream), and with its two temporaries (the FP32 x and the
+ * FP32 y) in a fixed array that the library reserves statically on every GPU that loads
+ * it, for as long as the process lives.
+ *   - Limit: n + m <= SPMV_NOALLOC_MAX_ELEMS (262144 FP32 elements, 1 MiB); larger
+ *     matrices get SPMV_ERR_ARG and nothing is launched.
+ *   - The first call on a device looks the array's device address up (once per device,
+ *     with that device current): make that first call before capturing a stream.
+ *   - All calls on a device share the array, and it keeps what the last call wrote.  Every
+ *     element a call reads it first writes, so nothing has to start at zero.  Calls whose
+ *     executions overlap on the GPU (other streams, other host threads) race on it:
+ *     serialise them.
+ * Calls no cudaMalloc, cudaFree or other allocating routine.
+ */
+#define SPMV_NOALLOC_MAX_ELEMS 262144
+int spmv_run_device_mixed_noalloc(spmv_handle * h, const double * d_x, double * d_y, void * stream);
+
 /* Waits for the handle's stream and returns the first device-side error, if any. */
 int spmv_sync(spmv_handle * h);
 

@@ -8,6 +8,8 @@ from ctypes import POINTER, c_char, c_char_p, c_double, c_int, c_int32, c_int64,
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "lib", "libspmv_b200.so")
 
+NOALLOC_MAX_ELEMS = 262144   # SPMV_NOALLOC_MAX_ELEMS
+
 # status codes
 SPMV_OK = 0
 SPMV_ERR_ARG = 1
@@ -75,6 +77,7 @@ SIGNATURES = {
     "spmv_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_run_device_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_run_f32": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "spmv_run_device_mixed_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_sync": (c_int, [c_void_p]),
     "spmv_get_info": (c_int, [c_void_p, POINTER(Info)]),
     "spmv_export": (c_int, [c_void_p, c_int32, c_void_p, POINTER(c_int64)]),

@@ -423,6 +423,17 @@ int spmv_run_f32(spmv_handle * H, const float * x, float * y)
 	return spmv::check_device_error(h);
 }
 
+int spmv_run_device_mixed_noalloc(spmv_handle * H, const double * d_x, double * d_y, void * stream)
+{
+	spmv::clear_error();
+	if (!H || (!d_x && H->h.n > 0) || (!d_y && H->h.m > 0)) {
+		spmv::set_error(SPMV_ERR_ARG, "null handle or vector");
+		return SPMV_ERR_ARG;
+	}
+	Handle & h = H->h;
+	return spmv::run_mixed_noalloc(h, d_x, d_y, stream ? (cudaStream_t) stream : h.stream);
+}
+
 int spmv_sync(spmv_handle * H)
 {
 	spmv::clear_error();

@@ -252,6 +252,57 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 	return SPMV_OK;
 }
 
+// ------------------------------------------------------------------ allocation-free entry
+// Scratch of spmv_run_device_mixed_noalloc: the FP32 copy of x followed by the FP32 y,
+// in one file-scope device array that every GPU loading this library holds until exit.
+static __device__ __align__(256) float g_mixed_scratch[SPMV_NOALLOC_MAX_ELEMS];
+
+// Device address of g_mixed_scratch per device, resolved once per device (with that
+// device current) by the first call on it.
+static float * g_mixed_scratch_addr[64];
+
+static int mixed_scratch(float ** out)
+{
+	int dev = 0;
+	SPMV_CUDA_TRY(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= 64) {
+		set_error(SPMV_ERR_ARG, "no-alloc entry: device ordinal %d out of range", dev);
+		return SPMV_ERR_ARG;
+	}
+	if (!g_mixed_scratch_addr[dev]) {
+		void * ptr = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&ptr, g_mixed_scratch);
+		if (e != cudaSuccess) {
+			set_error(SPMV_ERR_CUDA, "no-alloc entry: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+			return SPMV_ERR_CUDA;
+		}
+		g_mixed_scratch_addr[dev] = static_cast<float *>(ptr);
+	}
+	*out = g_mixed_scratch_addr[dev];
+	return SPMV_OK;
+}
+
+int run_mixed_noalloc(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
+{
+	if (h.desc.values != SPMV_VALUES_F32) {
+		set_error(SPMV_ERR_ARG, "no-alloc entry: the handle must store FP32 values (value type SPMV_VALUES_F32)");
+		return SPMV_ERR_ARG;
+	}
+	if (h.n + h.m > (int64_t) SPMV_NOALLOC_MAX_ELEMS) {
+		set_error(SPMV_ERR_ARG, "no-alloc entry: n + m = %lld exceeds its static scratch of %d FP32 elements",
+				(long long) (h.n + h.m), (int) SPMV_NOALLOC_MAX_ELEMS);
+		return SPMV_ERR_ARG;
+	}
+	float * scratch = nullptr;
+	SPMV_TRY(mixed_scratch(&scratch));
+	float * xf = scratch;            // x rounded to FP32: written in full before it is read
+	float * yf = scratch + h.n;      // FP32 y: every row is written by the SpMV kernel
+	SPMV_TRY(convert_vector_d2f(d_x, xf, h.n, s));
+	SPMV_TRY(launch_spmv_f32(h, xf, yf, s));
+	SPMV_TRY(convert_vector_f2d(yf, d_y, h.m, s));
+	return SPMV_OK;
+}
+
 int convert_vector_d2f(const double * in, float * out, int64_t n, cudaStream_t s)
 {
 	if (n > 0) {
