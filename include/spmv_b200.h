@@ -79,7 +79,9 @@ extern "C" {
  *                    threads per CTA), 0 = default.
  *   kernel           0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
- *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows).  default 0
+ *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);
+ *                    3: CTA staged kernel whose next-block x gather overlaps this block's
+ *                       rows (every format but DIV-RF; block_nnz <= 8 * threads).  default 0
  */
 typedef struct spmv_format_desc {
 	int32_t format;

@@ -408,7 +408,8 @@ int validate_csr(Handle & h)
 }
 
 // Kernel choice: the CTA staged kernel (0) by default; 1 = direct column-major kernel
-// (slices of >= 32 rows only), 2 = warp-autonomous staged kernel (slices of <= 32 rows).
+// (slices of >= 32 rows only), 2 = warp-autonomous staged kernel (slices of <= 32 rows),
+// 3 = CTA staged kernel with the next block's gather overlapping this block's rows.
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
@@ -422,6 +423,20 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 	if (k == 2)
 		return build_warp_chunks(h, d_P, U, V);
 	staged_defaults(h);
+	if ((k == 3 || k == 4) && h.desc.stages == 0)
+		h.stages = 3;
+	if (k == 4) {
+		// row warps: block_rows threads (default 64); at least one gather warp besides them
+		if (h.desc.threads == 0)
+			h.threads = 192;
+		h.row_threads = h.desc.block_rows > 0 ? h.desc.block_rows : 64;
+		if (h.row_threads % 32 != 0 || h.row_threads + 32 > h.threads || h.row_threads < V) {
+			set_error(SPMV_ERR_ARG, "warp-specialised kernel: block_rows %d must be a multiple of 32, at least the "
+					"slice height %d and leave a gather warp of %d threads", h.row_threads, V, h.threads);
+			return SPMV_ERR_ARG;
+		}
+		return build_blocks(h, d_P, U, h.row_threads / V);
+	}
 	int max_units = (h.desc.block_rows > 0 ? h.desc.block_rows : h.threads) / V;
 	if (max_units < 1)
 		max_units = 1;

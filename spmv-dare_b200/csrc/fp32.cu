@@ -100,10 +100,9 @@ __global__ void __launch_bounds__(F32_THREADS) f32_kernel(F32Args a)
 			if (b < a.nblocks)
 				issue_f32(a, b, s, smem, bars);
 		}
-	int it = 0;
-	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x, it++) {
-		const int s = it % a.stages;
-		const uint32_t parity = (uint32_t) ((it / a.stages) & 1);
+	int s = 0;
+	uint32_t parity = 0;
+	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
 		const StagedBlock d = a.blocks[b];
 		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
@@ -165,6 +164,10 @@ __global__ void __launch_bounds__(F32_THREADS) f32_kernel(F32Args a)
 			const int64_t nb = b + (int64_t) a.stages * gridDim.x;
 			if (nb < a.nblocks)
 				issue_f32(a, nb, s, smem, bars);
+		}
+		if (++s == a.stages) {
+			s = 0;
+			parity ^= 1u;
 		}
 	}
 }

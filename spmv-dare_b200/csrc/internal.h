@@ -86,7 +86,9 @@ struct Handle {
 	int stages = 0;
 	int threads = 256;           // threads per CTA of the staged kernel
 	size_t smem_bytes = 0;
-	int exec_kernel = 0;         // 0 CTA staged, 1 direct sliced, 2 warp-autonomous
+	int exec_kernel = 0;         // 0 CTA staged, 1 direct sliced, 2 warp-autonomous, 3 pipelined,
+	                             // 4 warp-specialised (gather warps + row warps)
+	int row_threads = 0;         // kernel 4: threads of the row warps (the rest gather)
 
 	// warp-autonomous kernel
 	WarpChunk * d_chunks = nullptr;

@@ -41,6 +41,7 @@ struct StagedArgs {
 	int stages;
 	int stage_bytes;
 	int exact;
+	int row_threads;         // warp-specialised kernel: threads of the row warps
 	int * err;
 };
 
@@ -95,9 +96,9 @@ __device__ __forceinline__ double csr_row(const double * __restrict__ vals, cons
 	}
 }
 
-__device__ __forceinline__ void staged_issue(const StagedArgs & a, int64_t b, int s, uint8_t * smem, uint64_t * bars)
+__device__ __forceinline__ void staged_issue_d(const StagedArgs & a, const StagedBlock & d, int s, uint8_t * smem,
+		uint64_t * bars)
 {
-	StagedBlock d = a.blocks[b];
 	if (d.units < 0 || d.elems == 0) {
 		mbar_arrive(&bars[s]);
 		return;
@@ -111,6 +112,12 @@ __device__ __forceinline__ void staged_issue(const StagedArgs & a, int64_t b, in
 	mbar_arrive_expect_tx(&bars[s], cnt * 12u);
 	bulk_g2s(sv, a.vals + e0, cnt * 8u, &bars[s]);
 	bulk_g2s(sc, a.cols + e0, cnt * 4u, &bars[s]);
+}
+
+__device__ __forceinline__ void staged_issue(const StagedArgs & a, int64_t b, int s, uint8_t * smem, uint64_t * bars)
+{
+	const StagedBlock d = a.blocks[b];
+	staged_issue_d(a, d, s, smem, bars);
 }
 
 // Deterministic CTA sum (fixed tree order).
@@ -227,6 +234,66 @@ __device__ __forceinline__ void staged_long_unit(const StagedArgs & a, const Sta
 	}
 }
 
+// Rows of one staged block whose gather is complete: one thread per row (CSR) or per
+// slice row (SLICED), in the reference order, operands in shared memory (`sv` values or
+// products, `xb` gathered x).  js0 / je0: bounds of this thread's first row relative to
+// the stage start, loaded ahead by the caller.
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void block_rows(const StagedArgs & a, const StagedBlock & d, const double * sv,
+		const double * xb, int js0, int je0)
+{
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	if (K == Kind::CSR) {
+		for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
+			const int64_t r = (int64_t) d.unit0 + u;
+			const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
+			const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
+			double sum = 0.0;
+			if (A == Arith::SEQ_SPLIT) {
+				#pragma unroll 4
+				for (int j = js; j < je; j++)
+					sum = __dadd_rn(sum, sv[j]);
+			} else if (A == Arith::SEQ_FMA) {
+				#pragma unroll 4
+				for (int j = js; j < je; j++)
+					sum = __fma_rn(sv[j], xb[j], sum);
+			} else {
+				double ln[L];
+				#pragma unroll
+				for (int l = 0; l < L; l++)
+					ln[l] = 0.0;
+				const int jv = js + ((je - js) & ~(L - 1));
+				for (int j = js; j < jv; j += L) {
+					#pragma unroll
+					for (int l = 0; l < L; l++)
+						ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
+				}
+				sum = lanes_reduce<L>(ln);
+				for (int j = jv; j < je; j++)
+					sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
+			}
+			a.y[r] = sum;
+		}
+	} else {
+		const int V = a.V;
+		const int nrow = d.units * V;
+		for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
+			const int64_t sl = (int64_t) d.unit0 + u / V;
+			const int lane = u % V;
+			const int64_t row = sl * V + lane;
+			if (row >= a.m)
+				continue;
+			const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
+			const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+			double acc = 0.0;
+			#pragma unroll 4
+			for (int k = 0; k < w; k++)
+				acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
+			a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+		}
+	}
+}
+
 // One staged block (or one long unit) of a staged kernel: gather, then rows in the
 // reference order.  `smem_stage` is the block's stage buffer, `xb` the gather buffer.
 template <Kind K, Arith A, int L, bool YMAP>
@@ -257,55 +324,7 @@ __device__ __forceinline__ void staged_block(const StagedArgs & a, const StagedB
 		}
 		__syncthreads();
 		// 2) one thread per row, reference order, operands in shared memory
-		if (K == Kind::CSR) {
-			for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
-				const int64_t r = (int64_t) d.unit0 + u;
-				const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
-				const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
-				double sum = 0.0;
-				if (A == Arith::SEQ_SPLIT) {
-					#pragma unroll 4
-					for (int j = js; j < je; j++)
-						sum = __dadd_rn(sum, sv[j]);
-				} else if (A == Arith::SEQ_FMA) {
-					#pragma unroll 4
-					for (int j = js; j < je; j++)
-						sum = __fma_rn(sv[j], xb[j], sum);
-				} else {
-					double ln[L];
-					#pragma unroll
-					for (int l = 0; l < L; l++)
-						ln[l] = 0.0;
-					const int jv = js + ((je - js) & ~(L - 1));
-					for (int j = js; j < jv; j += L) {
-						#pragma unroll
-						for (int l = 0; l < L; l++)
-							ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
-					}
-					sum = lanes_reduce<L>(ln);
-					for (int j = jv; j < je; j++)
-						sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
-				}
-				a.y[r] = sum;
-			}
-		} else {
-			const int V = a.V;
-			const int nrow = d.units * V;
-			for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
-				const int64_t sl = (int64_t) d.unit0 + u / V;
-				const int lane = u % V;
-				const int64_t row = sl * V + lane;
-				if (row >= a.m)
-					continue;
-				const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
-				const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
-				double acc = 0.0;
-				#pragma unroll 4
-				for (int k = 0; k < w; k++)
-					acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
-				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
-			}
-		}
+		block_rows<K, A, L, YMAP>(a, d, sv, xb, js0, je0);
 	} else {
 		staged_long_unit<K, A, L, YMAP>(a, d, xb);
 	}
@@ -324,31 +343,484 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a
 		mbar_fence_init();
 	}
 	__syncthreads();
+	// descriptors of the blocks in the ring, written by the issuing thread: the compute
+	// threads read them from shared memory instead of waiting on a global load per block
+	__shared__ StagedBlock sdesc[8];
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < a.stages; s++) {
 			int64_t b = (int64_t) blockIdx.x + (int64_t) s * gridDim.x;
-			if (b < a.nblocks)
-				staged_issue(a, b, s, smem, bars);
+			if (b < a.nblocks) {
+				const StagedBlock d = a.blocks[b];
+				sdesc[s] = d;
+				staged_issue_d(a, d, s, smem, bars);
+			}
 		}
 	}
 
-	int it = 0;
-	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x, it++) {
-		const int s = it % a.stages;
-		const uint32_t parity = (uint32_t) ((it / a.stages) & 1);
-		const StagedBlock d = a.blocks[b];
+	// ring slot and mbarrier phase of the current block, advanced incrementally (a runtime
+	// division per block costs more issue slots than the rest of the block's bookkeeping)
+	int s = 0;
+	uint32_t parity = 0;
+	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+		// the descriptor this iteration will issue, loaded now so its latency overlaps the block
+		const int64_t nb = b + (int64_t) a.stages * gridDim.x;
+		StagedBlock dnext{};
+		if (threadIdx.x == 0 && nb < a.nblocks)
+			dnext = a.blocks[nb];
 		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
 			if (threadIdx.x == 0)
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 			return;
 		}
+		const StagedBlock d = sdesc[s];
 		staged_block<K, A, L, YMAP>(a, d, smem + (size_t) s * a.stage_bytes, xb);
 		__syncthreads();
+		if (threadIdx.x == 0 && nb < a.nblocks) {
+			sdesc[s] = dnext;
+			staged_issue_d(a, dnext, s, smem, bars);
+		}
+		if (++s == a.stages) {
+			s = 0;
+			parity ^= 1u;
+		}
+	}
+}
+
+// ------------------------------------------------------------------ pipelined staged kernel
+// Same blocks, stage ring and per-row operation order as staged_kernel, but the x gather
+// of block i+1 is issued (into registers) before the rows of block i are summed, and
+// stored to shared memory after them, so the gather's L2 latency overlaps the dependent
+// add chains instead of following them.  Stage layout: values (8 B) | columns (4 B) |
+// gathered x (8 B; not for SEQ_SPLIT, whose products replace the values in place).
+// Requires block capacity <= PIPE_G * threads (one register slot per staged entry).
+constexpr int PIPE_G = 8;
+
+template <Kind K>
+__device__ __forceinline__ void first_row_bounds(const StagedArgs & a, const StagedBlock & d, int & js0, int & je0)
+{
+	js0 = 0;
+	je0 = 0;
+	if (K == Kind::CSR && d.units >= 0 && (int) threadIdx.x < d.units) {
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		const int64_t r = (int64_t) d.unit0 + threadIdx.x;
+		js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+		je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+	}
+}
+
+__device__ __forceinline__ void gather_load(const StagedArgs & a, const StagedBlock & d, const uint8_t * stage,
+		double (&xr)[PIPE_G])
+{
+	const int32_t * sc = reinterpret_cast<const int32_t *>(stage + (size_t) a.cap_al * 8);
+	const int off = d.elem0 & 3;
+	#pragma unroll
+	for (int k = 0; k < PIPE_G; k++) {
+		const int e = (int) threadIdx.x + k * (int) blockDim.x;
+		if (e < d.elems)
+			xr[k] = ldg(a.x + sc[off + e]);
+	}
+}
+
+template <Arith A>
+__device__ __forceinline__ void gather_store(const StagedArgs & a, const StagedBlock & d, uint8_t * stage,
+		const double (&xr)[PIPE_G])
+{
+	double * sv = reinterpret_cast<double *>(stage);
+	double * xg = reinterpret_cast<double *>(stage + (size_t) a.cap_al * 12);
+	const int off = d.elem0 & 3;
+	#pragma unroll
+	for (int k = 0; k < PIPE_G; k++) {
+		const int e = (int) threadIdx.x + k * (int) blockDim.x;
+		if (e < d.elems) {
+			if (A == Arith::SEQ_SPLIT)
+				sv[off + e] = __dmul_rn(sv[off + e], xr[k]);   // the reference's rounded product
+			else
+				xg[off + e] = xr[k];
+		}
+	}
+}
+
+template <Kind K, Arith A, int L, bool YMAP>
+__global__ void __launch_bounds__(STAGED_MAX_THREADS) pipe_kernel(StagedArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	uint64_t * bars = reinterpret_cast<uint64_t *>(smem + (size_t) a.stages * a.stage_bytes);
+	const int S = a.stages;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < S; s++)
+			mbar_init(&bars[s], 1);
+		mbar_fence_init();
+	}
+	__syncthreads();
+	if (threadIdx.x == 0)
+		for (int s = 0; s < S; s++) {
+			const int64_t b = (int64_t) blockIdx.x + (int64_t) s * gridDim.x;
+			if (b < a.nblocks)
+				staged_issue(a, b, s, smem, bars);
+		}
+	int64_t b = blockIdx.x;
+	if (b >= a.nblocks)
+		return;
+	StagedBlock d = a.blocks[b];
+	double xr[PIPE_G];
+	{
+		const bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitBudgetCycles);
+		if (__syncthreads_or(!ok)) {
+			if (threadIdx.x == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		if (d.units >= 0) {
+			gather_load(a, d, smem, xr);
+			gather_store<A>(a, d, smem, xr);
+		}
+		__syncthreads();
+	}
+	int s = 0;                          // ring slot of the current block
+	int ns = S > 1 ? 1 : 0;             // ring slot and mbarrier phase of the next block
+	uint32_t nparity = S > 1 ? 0u : 1u;
+	for (;;) {
+		uint8_t * stage = smem + (size_t) s * a.stage_bytes;
+		const int64_t nb = b + gridDim.x;
+		const bool has_next = nb < a.nblocks;
+		int js0, je0;
+		first_row_bounds<K>(a, d, js0, je0);
+		StagedBlock dn{};
+		uint8_t * nstage = smem + (size_t) ns * a.stage_bytes;
+		if (has_next) {
+			dn = a.blocks[nb];
+			const bool ok = mbar_wait_bounded(&bars[ns], nparity, kWaitBudgetCycles);
+			if (__syncthreads_or(!ok)) {
+				if (threadIdx.x == 0)
+					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				return;
+			}
+			if (dn.units >= 0)
+				gather_load(a, dn, nstage, xr);
+		}
+		if (d.units >= 0)
+			block_rows<K, A, L, YMAP>(a, d, reinterpret_cast<double *>(stage),
+					reinterpret_cast<const double *>(stage + (size_t) a.cap_al * 12), js0, je0);
+		else
+			staged_long_unit<K, A, L, YMAP>(a, d, reinterpret_cast<double *>(stage));  // no staged data: chunk buffer
+		if (has_next && dn.units >= 0)
+			gather_store<A>(a, dn, nstage, xr);
+		__syncthreads();
 		if (threadIdx.x == 0) {
-			int64_t nb = b + (int64_t) a.stages * gridDim.x;
-			if (nb < a.nblocks)
-				staged_issue(a, nb, s, smem, bars);
+			const int64_t fb = b + (int64_t) S * gridDim.x;
+			if (fb < a.nblocks)
+				staged_issue(a, fb, s, smem, bars);
+		}
+		if (!has_next)
+			break;
+		b = nb;
+		d = dn;
+		s = ns;
+		if (++ns == S) {
+			ns = 0;
+			nparity ^= 1u;
+		}
+	}
+}
+
+// Row bounds of row thread `t`'s row in block d, relative to the stage start (CSR).
+template <Kind K>
+__device__ __forceinline__ void first_row_bounds_t(const StagedArgs & a, const StagedBlock & d, int t, int & js0, int & je0)
+{
+	js0 = 0;
+	je0 = 0;
+	if (K == Kind::CSR && d.units >= 0 && t < d.units) {
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		const int64_t r = (int64_t) d.unit0 + t;
+		js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+		je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+	}
+}
+
+// block_rows for row thread t of nt (the block holds at most nt rows).
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock & d, const double * sv, const double * xb,
+		int js0, int je0, int t, int nt)
+{
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	if (K == Kind::CSR) {
+		if (t < d.units) {
+			const int64_t r = (int64_t) d.unit0 + t;
+			const int js = js0, je = je0;
+			double sum = 0.0;
+			if (A == Arith::SEQ_SPLIT) {
+				#pragma unroll 4
+				for (int j = js; j < je; j++)
+					sum = __dadd_rn(sum, sv[j]);
+			} else if (A == Arith::SEQ_FMA) {
+				#pragma unroll 4
+				for (int j = js; j < je; j++)
+					sum = __fma_rn(sv[j], xb[j], sum);
+			} else {
+				double ln[L];
+				#pragma unroll
+				for (int l = 0; l < L; l++)
+					ln[l] = 0.0;
+				const int jv = js + ((je - js) & ~(L - 1));
+				for (int j = js; j < jv; j += L) {
+					#pragma unroll
+					for (int l = 0; l < L; l++)
+						ln[l] = __fma_rn(sv[j + l], xb[j + l], ln[l]);
+				}
+				sum = lanes_reduce<L>(ln);
+				for (int j = jv; j < je; j++)
+					sum = __dadd_rn(sum, __dmul_rn(sv[j], xb[j]));
+			}
+			a.y[r] = sum;
+		}
+	} else {
+		const int V = a.V;
+		const int nrow = d.units * V;
+		for (int u = t; u < nrow; u += nt) {
+			const int64_t sl = (int64_t) d.unit0 + u / V;
+			const int lane = u % V;
+			const int64_t row = sl * V + lane;
+			if (row >= a.m)
+				continue;
+			const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
+			const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+			double acc = 0.0;
+			#pragma unroll 4
+			for (int k = 0; k < w; k++)
+				acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
+			a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+		}
+	}
+}
+
+// ------------------------------------------------------------------ warp-specialised staged kernel
+// The CTA's first warps gather (x loads, products or x into the stage), its last
+// `row_threads / 32` warps sum rows, so block k's rows run while block k+1 is gathered and
+// block k+2 is in flight.  Hand-offs: full[s] (bulk copy landed, with the block's
+// descriptor in sdesc[s]), prod[s] (every gather thread has written its entries; count =
+// gather threads).  The row warps give a stage back with a named barrier among themselves
+// and their first thread issues the stage's next copy.  Same blocks and per-row operation
+// order as staged_kernel; a block holds at most `row_threads` rows.
+__device__ __forceinline__ void named_bar_sync(int id, int n)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Named barrier over n threads that also returns whether any of them passed `pred` true
+// (so a decision to leave is taken by all of them together).
+__device__ __forceinline__ bool named_bar_or(int id, int n, bool pred)
+{
+	uint32_t out;
+	asm volatile(
+	    "{\n\t.reg .pred p, q;\n\t"
+	    "setp.ne.u32 p, %1, 0;\n\t"
+	    "bar.red.or.pred q, %2, %3, p;\n\t"
+	    "selp.u32 %0, 1, 0, q;\n\t}"
+	    : "=r"(out)
+	    : "r"((uint32_t) pred), "r"(id), "r"(n)
+	    : "memory");
+	return out != 0;
+}
+
+// A unit larger than one staged block, done by the row threads alone (rt of nr; named
+// barrier 1), chunked through the free stage buffer `buf` (cap_al doubles): one thread
+// continues each row in the reference order.
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void ws_long_unit(const StagedArgs & a, const StagedBlock & d, double * buf, int rt, int nr)
+{
+	const int half = a.cap_al / 2;
+	double * cv = buf;
+	double * cx = buf + half;
+	if (K == Kind::CSR) {
+		const int64_t r = d.unit0;
+		const int64_t js = a.ptr[r], je = a.ptr[r + 1];
+		const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
+		double sum = 0.0;
+		double lane[L];
+		#pragma unroll
+		for (int l = 0; l < L; l++)
+			lane[l] = 0.0;
+		for (int64_t c0 = js; c0 < je; c0 += half) {
+			const int cnt = (int) ((je - c0) < half ? (je - c0) : half);
+			for (int e = rt; e < cnt; e += nr) {
+				const double v = a.vals[c0 + e];
+				const double xv = ldg(a.x + a.cols[c0 + e]);
+				if (A == Arith::SEQ_SPLIT) {
+					cv[e] = __dmul_rn(v, xv);
+				} else {
+					cv[e] = v;
+					cx[e] = xv;
+				}
+			}
+			named_bar_sync(1, nr);
+			if (rt == 0) {
+				if (A == Arith::SEQ_SPLIT) {
+					#pragma unroll 4
+					for (int e = 0; e < cnt; e++)
+						sum = __dadd_rn(sum, cv[e]);
+				} else {
+					for (int e = 0; e < cnt; e++) {
+						const int64_t j = c0 + e;
+						if (A == Arith::LANES_FMA) {
+							if (j < jv) {
+								const int l = (int) ((j - js) & (L - 1));
+								#pragma unroll
+								for (int q = 0; q < L; q++)
+									if (q == l)
+										lane[q] = __fma_rn(cv[e], cx[e], lane[q]);
+							} else {
+								if (j == jv)
+									sum = lanes_reduce<L>(lane);
+								sum = __dadd_rn(sum, __dmul_rn(cv[e], cx[e]));
+							}
+						} else {
+							sum = __fma_rn(cv[e], cx[e], sum);
+						}
+					}
+				}
+			}
+			named_bar_sync(1, nr);
+		}
+		if (rt == 0) {
+			if (A == Arith::LANES_FMA && jv == je)
+				sum = lanes_reduce<L>(lane);
+			a.y[r] = sum;
+		}
+	} else {
+		const int V = a.V;
+		const int64_t sl = d.unit0;
+		const int64_t p0 = a.ptr[sl];
+		const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+		const int kc = half / V > 0 ? half / V : 1;
+		double acc = 0.0;
+		for (int k0 = 0; k0 < w; k0 += kc) {
+			const int kn = (w - k0) < kc ? (w - k0) : kc;
+			const int cnt = kn * V;
+			const int64_t base = p0 + (int64_t) k0 * V;
+			for (int e = rt; e < cnt; e += nr) {
+				cv[e] = a.vals[base + e];
+				cx[e] = ldg(a.x + a.cols[base + e]);
+			}
+			named_bar_sync(1, nr);
+			if (rt < V)
+				for (int k = 0; k < kn; k++)
+					acc = __fma_rn(cv[k * V + rt], cx[k * V + rt], acc);
+			named_bar_sync(1, nr);
+		}
+		if (rt < V) {
+			const int64_t row = sl * V + rt;
+			if (row < a.m)
+				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+		}
+	}
+}
+
+template <Kind K, Arith A, int L, bool YMAP>
+__global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	__shared__ StagedBlock sdesc[8];
+	const int S = a.stages;
+	uint64_t * full = reinterpret_cast<uint64_t *>(smem + (size_t) S * a.stage_bytes);
+	uint64_t * prod = full + S;
+	const int nr = a.row_threads;
+	const int ng = (int) blockDim.x - nr;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < S; s++) {
+			mbar_init(&full[s], 1);
+			mbar_init(&prod[s], (uint32_t) ng);
+		}
+		mbar_fence_init();
+	}
+	__syncthreads();
+	int s = 0;
+	uint32_t parity = 0;
+	if ((int) threadIdx.x < ng) {
+		// ---- gather warps
+		const int gt = threadIdx.x;
+		for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+			if (!mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles)) {
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				return;
+			}
+			const StagedBlock d = sdesc[s];
+			if (d.units >= 0) {
+				uint8_t * st = smem + (size_t) s * a.stage_bytes;
+				double * sv = reinterpret_cast<double *>(st);
+				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cap_al * 8);
+				double * xg = reinterpret_cast<double *>(st + (size_t) a.cap_al * 12);
+				const int off = d.elem0 & 3;
+				// 4 independent loads in flight per thread: the column loads of a group are
+				// all issued before any store of the group, so the x loads overlap
+				for (int e0 = gt; e0 < d.elems; e0 += 4 * ng) {
+					double xv[4];
+					#pragma unroll
+					for (int k = 0; k < 4; k++) {
+						const int e = e0 + k * ng;
+						if (e < d.elems)
+							xv[k] = ldg(a.x + sc[off + e]);
+					}
+					#pragma unroll
+					for (int k = 0; k < 4; k++) {
+						const int e = e0 + k * ng;
+						if (e < d.elems) {
+							if (A == Arith::SEQ_SPLIT)
+								sv[off + e] = __dmul_rn(sv[off + e], xv[k]);   // the reference's rounded product
+							else
+								xg[off + e] = xv[k];
+						}
+					}
+				}
+			}
+			mbar_arrive(&prod[s]);
+			if (++s == S) {
+				s = 0;
+				parity ^= 1u;
+			}
+		}
+		return;
+	}
+	// ---- row warps
+	const int rt = (int) threadIdx.x - ng;
+	if (rt == 0)
+		for (int q = 0; q < S; q++) {
+			const int64_t b = (int64_t) blockIdx.x + (int64_t) q * gridDim.x;
+			if (b < a.nblocks) {
+				const StagedBlock d = a.blocks[b];
+				sdesc[q] = d;
+				staged_issue_d(a, d, q, smem, full);
+			}
+		}
+	named_bar_sync(1, nr);
+	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+		const int64_t nb = b + (int64_t) S * gridDim.x;
+		StagedBlock dnext{};
+		if (rt == 0 && nb < a.nblocks)
+			dnext = a.blocks[nb];
+		const StagedBlock d = sdesc[s];
+		int js0 = 0, je0 = 0;
+		first_row_bounds_t<K>(a, d, rt, js0, je0);
+		const bool ok = mbar_wait_bounded(&prod[s], parity, kWaitBudgetCycles);
+		if (named_bar_or(1, nr, !ok)) {      // all row threads leave together
+			if (rt == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		uint8_t * st = smem + (size_t) s * a.stage_bytes;
+		if (d.units >= 0)
+			rows_t<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(st),
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), js0, je0, rt, nr);
+		else
+			ws_long_unit<K, A, L, YMAP>(a, d, reinterpret_cast<double *>(st), rt, nr);
+		named_bar_sync(1, nr);
+		if (rt == 0 && nb < a.nblocks) {
+			sdesc[s] = dnext;
+			staged_issue_d(a, dnext, s, smem, full);
+		}
+		if (++s == S) {
+			s = 0;
+			parity ^= 1u;
 		}
 	}
 }
@@ -399,9 +871,9 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) batch_kernel(BatchArgs b)
 	if (threadIdx.x == 0)
 		for (int s = 0; s < b.stages; s++)
 			batch_issue(b, (int64_t) atomicAdd(b.counter, 1ULL), s, smem, bars, claim);
-	for (int it = 0;; it++) {
-		const int s = it % b.stages;
-		const uint32_t parity = (uint32_t) ((it / b.stages) & 1);
+	int s = 0;
+	uint32_t parity = 0;
+	for (;; ) {
 		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
 			if (threadIdx.x == 0)
@@ -435,6 +907,10 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) batch_kernel(BatchArgs b)
 		__syncthreads();
 		if (threadIdx.x == 0)
 			batch_issue(b, (int64_t) atomicAdd(b.counter, 1ULL), s, smem, bars, claim);
+		if (++s == b.stages) {
+			s = 0;
+			parity ^= 1u;
+		}
 	}
 }
 
@@ -520,6 +996,60 @@ StagedFn pick_staged(const Handle & h)
 	return nullptr;
 }
 
+// The pipelined kernel instance of a handle's format / lane count.
+StagedFn pick_pipe(const Handle & h)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_CSR_NAIVE)
+		return pipe_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+	if (fmt == SPMV_FMT_CSR_VEC) {
+		switch (h.desc.vec_len) {
+		case 1: return pipe_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
+		case 2: return pipe_kernel<Kind::CSR, Arith::LANES_FMA, 2, false>;
+		case 4: return pipe_kernel<Kind::CSR, Arith::LANES_FMA, 4, false>;
+		case 8: return pipe_kernel<Kind::CSR, Arith::LANES_FMA, 8, false>;
+		case 16: return pipe_kernel<Kind::CSR, Arith::LANES_FMA, 16, false>;
+		}
+		return nullptr;
+	}
+	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
+		return pipe_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+	if (fmt == SPMV_FMT_SELL)
+		return pipe_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+	return nullptr;
+}
+
+// The warp-specialised kernel instance of a handle's format / lane count.
+StagedFn pick_ws(const Handle & h)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_CSR_NAIVE)
+		return ws_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+	if (fmt == SPMV_FMT_CSR_VEC) {
+		switch (h.desc.vec_len) {
+		case 1: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
+		case 2: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 2, false>;
+		case 4: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 4, false>;
+		case 8: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 8, false>;
+		case 16: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 16, false>;
+		}
+		return nullptr;
+	}
+	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
+		return ws_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+	if (fmt == SPMV_FMT_SELL)
+		return ws_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+	return nullptr;
+}
+
+// Bytes of one stage of the pipelined kernel (values, columns, and gathered x unless the
+// products are formed in place).
+int pipe_stage_bytes(int format, int cap_al)
+{
+	const int per = (format == SPMV_FMT_CSR_NAIVE) ? 12 : 20;
+	return (int) (ceil_div((int64_t) cap_al * per, 128) * 128);
+}
+
 }  // namespace
 
 int batch_launch(const BatchArgs & b, int grid, int threads, size_t smem, cudaStream_t s)
@@ -544,6 +1074,75 @@ int batch_occupancy(int threads, size_t smem, int * per_sm)
 // Grid / shared-memory geometry of the staged kernel for this handle.
 int staged_geometry(Handle & h)
 {
+	if (h.exec_kernel == 4) {
+		const int cap_al = h.block_cap + 8;
+		const int stage_bytes = pipe_stage_bytes(h.desc.format, cap_al);
+		const int max_stages = (220 * 1024 - 128) / stage_bytes;
+		if (max_stages < 2) {
+			set_error(SPMV_ERR_ARG, "warp-specialised kernel: staging block of %d entries exceeds shared memory",
+					h.block_cap);
+			return SPMV_ERR_ARG;
+		}
+		if (h.stages > max_stages)
+			h.stages = max_stages;
+		if (h.stages < 2)
+			h.stages = 2;
+		h.smem_bytes = (size_t) h.stages * stage_bytes + (size_t) h.stages * 16;
+		StagedFn kern = pick_ws(h);
+		if (!kern) {
+			set_error(SPMV_ERR_ARG, "no warp-specialised kernel for format %d with vec_len %d", h.desc.format,
+					h.desc.vec_len);
+			return SPMV_ERR_ARG;
+		}
+		SPMV_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) h.smem_bytes));
+		int ctas = h.desc.ctas_per_sm > 0 ? h.desc.ctas_per_sm : 0;
+		if (ctas == 0) {
+			int per_sm = 0;
+			SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h.threads, h.smem_bytes));
+			ctas = per_sm > 0 ? per_sm : 1;
+		}
+		int64_t g = (int64_t) h.num_sms * ctas;
+		if (g > h.num_blocks)
+			g = h.num_blocks;
+		h.grid = (int) (g > 0 ? g : 1);
+		return SPMV_OK;
+	}
+	if (h.exec_kernel == 3) {
+		const int cap_al = h.block_cap + 8;
+		if (h.block_cap > PIPE_G * h.threads) {
+			set_error(SPMV_ERR_ARG, "pipelined kernel: %d staged entries exceed %d per thread x %d threads",
+					h.block_cap, PIPE_G, h.threads);
+			return SPMV_ERR_ARG;
+		}
+		const int stage_bytes = pipe_stage_bytes(h.desc.format, cap_al);
+		const int max_stages = (220 * 1024 - 64) / stage_bytes;
+		if (max_stages < 2) {
+			set_error(SPMV_ERR_ARG, "pipelined kernel: staging block of %d entries exceeds shared memory", h.block_cap);
+			return SPMV_ERR_ARG;
+		}
+		if (h.stages > max_stages)
+			h.stages = max_stages;
+		if (h.stages < 2)
+			h.stages = 2;
+		h.smem_bytes = (size_t) h.stages * stage_bytes + 64;
+		StagedFn kern = pick_pipe(h);
+		if (!kern) {
+			set_error(SPMV_ERR_ARG, "no pipelined kernel for format %d with vec_len %d", h.desc.format, h.desc.vec_len);
+			return SPMV_ERR_ARG;
+		}
+		SPMV_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) h.smem_bytes));
+		int ctas = h.desc.ctas_per_sm > 0 ? h.desc.ctas_per_sm : 0;
+		if (ctas == 0) {
+			int per_sm = 0;
+			SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h.threads, h.smem_bytes));
+			ctas = per_sm > 0 ? per_sm : 1;
+		}
+		int64_t g = (int64_t) h.num_sms * ctas;
+		if (g > h.num_blocks)
+			g = h.num_blocks;
+		h.grid = (int) (g > 0 ? g : 1);
+		return SPMV_OK;
+	}
 	const int cap_al = h.block_cap + 8;
 	const int stage_bytes = (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
 	// keep the pipeline inside the 227 KB a CTA may use (fewer stages for large blocks)
@@ -652,6 +1251,14 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
 	}
 	StagedFn kern = pick_staged(h);
+	if (h.exec_kernel == 3) {
+		kern = pick_pipe(h);
+		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
+	} else if (h.exec_kernel == 4) {
+		kern = pick_ws(h);
+		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
+		a.row_threads = h.row_threads;
+	}
 	kern<<<h.grid, h.threads, h.smem_bytes, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;

@@ -106,10 +106,9 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 	#pragma unroll
 	for (int l = 0; l < L; l++)
 		ln[l] = 0.0;
-	int it = 0;
-	for (int64_t c = cb; c < ce; c++, it++) {
-		const int s = it % a.stages;
-		const uint32_t parity = (uint32_t) ((it / a.stages) & 1);
+	int s = 0;
+	uint32_t parity = 0;
+	for (int64_t c = cb; c < ce; c++) {
 		const WarpChunk d = a.chunks[c];
 		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (!__all_sync(0xffffffffu, ok)) {
@@ -247,6 +246,10 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 		__syncwarp();
 		if (lane == 0 && c + a.stages < ce)
 			warp_issue(a, c + a.stages, wsm, &bars[s], s);
+		if (++s == a.stages) {
+			s = 0;
+			parity ^= 1u;
+		}
 	}
 }
 

@@ -106,6 +106,56 @@ def test_staging_geometry_does_not_change_results(sb, fmt, block_nnz, stages):
         assert _eq_bits(y, g[f"y_{fmt}"]).size == 0, (name, fmt, block_nnz)
 
 
+@pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s"])
+@pytest.mark.parametrize("threads,block_nnz,stages", [(256, 64, 2), (128, 256, 3), (256, 0, 0), (512, 2048, 4)])
+def test_pipelined_kernel_matches_reference(sb, orc, fmt, threads, block_nnz, stages):
+    """Kernel 3 (next block's gather overlapping this block's rows): same y bits as the
+    reference for every golden case; tiny blocks force the long-unit path."""
+    for name in golden_names():
+        g = load_golden(name)
+        mf = _mk(sb, g, fmt, kernel=3, threads=threads, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        if fmt == "sell_c_s":
+            arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], 32, 512)
+            ref = orc.sellcs_spmv(arr, mf.m, 32, g["x"])
+        else:
+            ref = g[f"y_{fmt}"]
+        assert _eq_bits(y, ref).size == 0, (name, fmt, threads, block_nnz, stages)
+
+
+@pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s"])
+@pytest.mark.parametrize("threads,block_rows,block_nnz,stages",
+                         [(0, 0, 0, 0), (96, 64, 64, 2), (256, 32, 256, 3), (512, 128, 2048, 4)])
+def test_warp_specialised_kernel_matches_reference(sb, orc, fmt, threads, block_rows, block_nnz, stages):
+    """Kernel 4 (gather warps + row warps): same y bits as the reference for every golden
+    case; 64-entry blocks force the long-unit path of the row warps."""
+    for name in golden_names():
+        g = load_golden(name)
+        mf = _mk(sb, g, fmt, kernel=4, threads=threads, block_rows=block_rows, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        if fmt == "sell_c_s":
+            arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], 32, 512)
+            ref = orc.sellcs_spmv(arr, mf.m, 32, g["x"])
+        else:
+            ref = g[f"y_{fmt}"]
+        assert _eq_bits(y, ref).size == 0, (name, fmt, threads, block_rows, block_nnz, stages)
+
+
+def test_warp_specialised_kernel_rejects_bad_split(sb):
+    g = load_golden("hand6")
+    for kw in [dict(threads=64, block_rows=64), dict(threads=128, block_rows=48)]:
+        with pytest.raises(sb.SpmvError):
+            _mk(sb, g, "csr_naive", kernel=4, **kw)
+    with pytest.raises(sb.SpmvError):       # slices of 32 rows need at least 32 row threads... and 64 > 32
+        _mk(sb, g, "sell_c_s", kernel=4, threads=64, block_rows=32, sellcs_c=64, sellcs_sigma=64)
+
+
+def test_pipelined_kernel_rejects_oversized_blocks(sb):
+    g = load_golden("hand6")
+    with pytest.raises(sb.SpmvError):
+        _mk(sb, g, "csr_naive", kernel=3, threads=64, block_nnz=1024)
+
+
 def test_non_exact_long_rows_within_tolerance(sb, orc):
     g = load_golden("long_rows_60")
     mf = _mk(sb, g, "csr_naive", exact=0, block_nnz=512)
