@@ -72,16 +72,21 @@ extern "C" {
  *   div_tolerance        DIV_VC_TOLERANCE, lossy value rounding (config.sh:123). default 0
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
- *                        reduced in parallel (tolerance parity).                   default 1
+ *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,
+ *                        kernel 4 always sums in order).                           default 1
  *   values               SPMV_VALUES_F64 or SPMV_VALUES_F32.                       default F64
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
  *                    threads per CTA), 0 = default.
- *   kernel           0: CTA staged kernel (bulk copy + shared-memory gather, every format);
+ *   kernel          -1: the format's default (4 for csr_naive, 0 otherwise);
+ *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
  *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);
  *                    3: CTA staged kernel whose next-block x gather overlaps this block's
- *                       rows (every format but DIV-RF; block_nnz <= 8 * threads).  default 0
+ *                       rows (every format but DIV-RF; block_nnz <= 8 * threads);
+ *                    4: warp-specialised staged kernel: gather warps and block_rows row
+ *                       threads (default 64 of 160) work on consecutive blocks at once
+ *                       (every format but DIV-RF).  default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;

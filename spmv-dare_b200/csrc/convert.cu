@@ -42,7 +42,10 @@ __global__ void validate_csr_kernel(const int32_t * rp, const int32_t * ci, int6
 // `max_units` units, inside tiles of BLOCK_TILE_UNITS units (one thread per tile).
 // A unit larger than `cap` becomes a block of its own, marked long (units = -1).
 template <bool WRITE>
-__global__ void blocks_kernel(const int32_t * P, int64_t U, int cap, int max_units, int64_t * counts,
+// chunk > 0: a unit longer than `cap` becomes consecutive chunk blocks of `chunk` entries
+// (units = -1 - flags, flags bit 0 = first chunk, bit 1 = last chunk) instead of one long
+// block (units = -1, elems = the unit's length).
+__global__ void blocks_kernel(const int32_t * P, int64_t U, int cap, int max_units, int chunk, int64_t * counts,
 		const int64_t * offs, StagedBlock * out)
 {
 	int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,9 +58,19 @@ __global__ void blocks_kernel(const int32_t * P, int64_t U, int cap, int max_uni
 	while (u < end) {
 		int64_t len = (int64_t) P[u + 1] - P[u];
 		if (len > cap) {
-			if (WRITE)
-				out[o + nb] = StagedBlock{(int32_t) u, -1, P[u], (int32_t) len};
-			nb++;
+			if (chunk > 0) {
+				for (int64_t c0 = 0; c0 < len; c0 += chunk) {
+					const int64_t cl = (len - c0) < chunk ? (len - c0) : chunk;
+					const int flags = (c0 == 0 ? 1 : 0) | (c0 + cl == len ? 2 : 0);
+					if (WRITE)
+						out[o + nb] = StagedBlock{(int32_t) u, -1 - flags, (int32_t) (P[u] + c0), (int32_t) cl};
+					nb++;
+				}
+			} else {
+				if (WRITE)
+					out[o + nb] = StagedBlock{(int32_t) u, -1, P[u], (int32_t) len};
+				nb++;
+			}
 			u++;
 			continue;
 		}
@@ -74,7 +87,7 @@ __global__ void blocks_kernel(const int32_t * P, int64_t U, int cap, int max_uni
 		counts[t] = nb;
 }
 
-int build_blocks(Handle & h, const int32_t * d_P, int64_t U, int max_units)
+int build_blocks(Handle & h, const int32_t * d_P, int64_t U, int max_units, int chunk)
 {
 	cudaStream_t s = h.stream;
 	int64_t tiles = ceil_div(U, BLOCK_TILE_UNITS);
@@ -86,7 +99,7 @@ int build_blocks(Handle & h, const int32_t * d_P, int64_t U, int max_units)
 	SPMV_TRY(counts.alloc(tiles * sizeof(int64_t), s));
 	SPMV_TRY(offs.alloc((tiles + 1) * sizeof(int64_t), s));
 	unsigned grid = (unsigned) ceil_div(tiles, 128);
-	blocks_kernel<false><<<grid, 128, 0, s>>>(d_P, U, h.block_cap, max_units, counts.as<int64_t>(), nullptr, nullptr);
+	blocks_kernel<false><<<grid, 128, 0, s>>>(d_P, U, h.block_cap, max_units, chunk, counts.as<int64_t>(), nullptr, nullptr);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	SPMV_TRY(scan_exclusive(counts.as<int64_t>(), offs.as<int64_t>(), tiles, s));
 	int64_t nb = 0;
@@ -94,7 +107,7 @@ int build_blocks(Handle & h, const int32_t * d_P, int64_t U, int max_units)
 	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
 	h.num_blocks = nb;
 	SPMV_TRY(h.alloc(&h.d_blocks, nb));
-	blocks_kernel<true><<<grid, 128, 0, s>>>(d_P, U, h.block_cap, max_units, nullptr, offs.as<int64_t>(), h.d_blocks);
+	blocks_kernel<true><<<grid, 128, 0, s>>>(d_P, U, h.block_cap, max_units, chunk, nullptr, offs.as<int64_t>(), h.d_blocks);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return staged_geometry(h);
 }
@@ -407,12 +420,16 @@ int validate_csr(Handle & h)
 	return SPMV_OK;
 }
 
-// Kernel choice: the CTA staged kernel (0) by default; 1 = direct column-major kernel
-// (slices of >= 32 rows only), 2 = warp-autonomous staged kernel (slices of <= 32 rows),
-// 3 = CTA staged kernel with the next block's gather overlapping this block's rows.
+// Kernel choice: -1 = the format's default (the warp-specialised kernel for csr_naive, the
+// CTA staged kernel otherwise, the fastest of each on the 4M-row configuration); 0 = CTA
+// staged kernel; 1 = direct column-major kernel (slices of >= 32 rows only); 2 =
+// warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
+// block's gather overlapping this block's rows; 4 = warp-specialised staged kernel.
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
+	if (k < 0)
+		k = (h.desc.format == SPMV_FMT_CSR_NAIVE) ? 4 : 0;
 	if (k == 1 && V < 32)
 		k = 0;
 	if (k == 2 && V > 32)
@@ -428,19 +445,24 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 	if (k == 4) {
 		// row warps: block_rows threads (default 64); at least one gather warp besides them
 		if (h.desc.threads == 0)
-			h.threads = 192;
+			h.threads = 160;              // 3 gather warps + 2 row warps
 		h.row_threads = h.desc.block_rows > 0 ? h.desc.block_rows : 64;
 		if (h.row_threads % 32 != 0 || h.row_threads + 32 > h.threads || h.row_threads < V) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: block_rows %d must be a multiple of 32, at least the "
 					"slice height %d and leave a gather warp of %d threads", h.row_threads, V, h.threads);
 			return SPMV_ERR_ARG;
 		}
-		return build_blocks(h, d_P, U, h.row_threads / V);
+		if (h.block_cap < V) {
+			set_error(SPMV_ERR_ARG, "warp-specialised kernel: block_nnz %d below the slice height %d", h.block_cap, V);
+			return SPMV_ERR_ARG;
+		}
+		// units longer than a block: chunks of whole slice columns, summed in order by one CTA
+		return build_blocks(h, d_P, U, h.row_threads / V, (h.block_cap / V) * V);
 	}
 	int max_units = (h.desc.block_rows > 0 ? h.desc.block_rows : h.threads) / V;
 	if (max_units < 1)
 		max_units = 1;
-	return build_blocks(h, d_P, U, max_units);
+	return build_blocks(h, d_P, U, max_units, 0);
 }
 
 int convert_csr(Handle & h)

@@ -80,6 +80,7 @@ struct Handle {
 
 	// staged kernel
 	StagedBlock * d_blocks = nullptr;
+	int64_t * d_cta_ranges = nullptr;  // kernel 4: first block of each CTA's contiguous range (grid + 1)
 	int64_t num_blocks = 0;
 	int grid = 0;
 	int block_cap = 0;           // staging capacity in entries

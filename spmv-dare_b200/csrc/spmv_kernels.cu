@@ -19,6 +19,7 @@
 //                   (coalesced), fused multiply-add over the slice width as vfmacc does
 //                   (sellcs_mv_d, sell-C-s/sellcs_mv_kernels_epi.c:209-317).
 #include "internal.h"
+#include "primitives.cuh"
 
 namespace spmv {
 
@@ -42,6 +43,7 @@ struct StagedArgs {
 	int stage_bytes;
 	int exact;
 	int row_threads;         // warp-specialised kernel: threads of the row warps
+	const int64_t * ranges;  // warp-specialised kernel: each CTA's contiguous block range
 	int * err;
 };
 
@@ -600,8 +602,9 @@ __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock &
 // block k+2 is in flight.  Hand-offs: full[s] (bulk copy landed, with the block's
 // descriptor in sdesc[s]), prod[s] (every gather thread has written its entries; count =
 // gather threads).  The row warps give a stage back with a named barrier among themselves
-// and their first thread issues the stage's next copy.  Same blocks and per-row operation
-// order as staged_kernel; a block holds at most `row_threads` rows.
+// and their first thread issues the stage's next copy.  Same per-row operation order as
+// staged_kernel; a block holds at most `row_threads` rows, and a unit longer than a block
+// is a run of chunk blocks.  Each CTA walks a contiguous range of the block table.
 __device__ __forceinline__ void named_bar_sync(int id, int n)
 {
 	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
@@ -623,97 +626,151 @@ __device__ __forceinline__ bool named_bar_or(int id, int n, bool pred)
 	return out != 0;
 }
 
-// A unit larger than one staged block, done by the row threads alone (rt of nr; named
-// barrier 1), chunked through the free stage buffer `buf` (cap_al doubles): one thread
-// continues each row in the reference order.
-template <Kind K, Arith A, int L, bool YMAP>
-__device__ __forceinline__ void ws_long_unit(const StagedArgs & a, const StagedBlock & d, double * buf, int rt, int nr)
+// Bulk copy of a block's entries for the warp-specialised kernel (chunk blocks of long
+// units included; only an empty block completes the stage without a copy).
+__device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
 {
-	const int half = a.cap_al / 2;
-	double * cv = buf;
-	double * cx = buf + half;
+	if (d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
+	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 12u);
+	bulk_g2s(sv, a.vals + e0, cnt * 8u, &bars[s]);
+	bulk_g2s(sc, a.cols + e0, cnt * 4u, &bars[s]);
+}
+
+// One chunk block of a unit longer than a staged block (units = -1 - flags; bit 0: first
+// chunk, bit 1: last).  The unit's running state (sum, lanes) lives in the row thread's
+// registers between consecutive chunks, which the same CTA processes in order, so every
+// row is still summed by one thread in the reference order.
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void ws_chunk(const StagedArgs & a, const StagedBlock & d, const double * sv, const double * xg,
+		int rt, double & acc, double (&ln)[L])
+{
+	const int flags = -d.units - 1;
+	const int off = d.elem0 & 3;
 	if (K == Kind::CSR) {
+		if (rt != 0)
+			return;
 		const int64_t r = d.unit0;
-		const int64_t js = a.ptr[r], je = a.ptr[r + 1];
-		const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
-		double sum = 0.0;
-		double lane[L];
-		#pragma unroll
-		for (int l = 0; l < L; l++)
-			lane[l] = 0.0;
-		for (int64_t c0 = js; c0 < je; c0 += half) {
-			const int cnt = (int) ((je - c0) < half ? (je - c0) : half);
-			for (int e = rt; e < cnt; e += nr) {
-				const double v = a.vals[c0 + e];
-				const double xv = ldg(a.x + a.cols[c0 + e]);
-				if (A == Arith::SEQ_SPLIT) {
-					cv[e] = __dmul_rn(v, xv);
+		if (flags & 1) {
+			acc = 0.0;
+			#pragma unroll
+			for (int l = 0; l < L; l++)
+				ln[l] = 0.0;
+		}
+		if (A == Arith::SEQ_SPLIT) {
+			#pragma unroll 4
+			for (int e = 0; e < d.elems; e++)
+				acc = __dadd_rn(acc, sv[off + e]);
+		} else if (A == Arith::SEQ_FMA) {
+			#pragma unroll 4
+			for (int e = 0; e < d.elems; e++)
+				acc = __fma_rn(sv[off + e], xg[off + e], acc);
+		} else {
+			const int64_t js = a.ptr[r], je = a.ptr[r + 1];
+			const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
+			for (int e = 0; e < d.elems; e++) {
+				const int64_t j = (int64_t) d.elem0 + e;
+				if (j < jv) {
+					const int l = (int) ((j - js) & (L - 1));
+					#pragma unroll
+					for (int q = 0; q < L; q++)
+						if (q == l)
+							ln[q] = __fma_rn(sv[off + e], xg[off + e], ln[q]);
 				} else {
-					cv[e] = v;
-					cx[e] = xv;
+					if (j == jv)
+						acc = lanes_reduce<L>(ln);
+					acc = __dadd_rn(acc, __dmul_rn(sv[off + e], xg[off + e]));
 				}
 			}
-			named_bar_sync(1, nr);
-			if (rt == 0) {
-				if (A == Arith::SEQ_SPLIT) {
-					#pragma unroll 4
-					for (int e = 0; e < cnt; e++)
-						sum = __dadd_rn(sum, cv[e]);
-				} else {
-					for (int e = 0; e < cnt; e++) {
-						const int64_t j = c0 + e;
-						if (A == Arith::LANES_FMA) {
-							if (j < jv) {
-								const int l = (int) ((j - js) & (L - 1));
-								#pragma unroll
-								for (int q = 0; q < L; q++)
-									if (q == l)
-										lane[q] = __fma_rn(cv[e], cx[e], lane[q]);
-							} else {
-								if (j == jv)
-									sum = lanes_reduce<L>(lane);
-								sum = __dadd_rn(sum, __dmul_rn(cv[e], cx[e]));
-							}
-						} else {
-							sum = __fma_rn(cv[e], cx[e], sum);
-						}
-					}
-				}
-			}
-			named_bar_sync(1, nr);
+			if ((flags & 2) && jv == je)
+				acc = lanes_reduce<L>(ln);
 		}
-		if (rt == 0) {
-			if (A == Arith::LANES_FMA && jv == je)
-				sum = lanes_reduce<L>(lane);
-			a.y[r] = sum;
-		}
+		if (flags & 2)
+			a.y[r] = acc;
 	} else {
 		const int V = a.V;
-		const int64_t sl = d.unit0;
-		const int64_t p0 = a.ptr[sl];
-		const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
-		const int kc = half / V > 0 ? half / V : 1;
-		double acc = 0.0;
-		for (int k0 = 0; k0 < w; k0 += kc) {
-			const int kn = (w - k0) < kc ? (w - k0) : kc;
-			const int cnt = kn * V;
-			const int64_t base = p0 + (int64_t) k0 * V;
-			for (int e = rt; e < cnt; e += nr) {
-				cv[e] = a.vals[base + e];
-				cx[e] = ldg(a.x + a.cols[base + e]);
-			}
-			named_bar_sync(1, nr);
-			if (rt < V)
-				for (int k = 0; k < kn; k++)
-					acc = __fma_rn(cv[k * V + rt], cx[k * V + rt], acc);
-			named_bar_sync(1, nr);
-		}
-		if (rt < V) {
-			const int64_t row = sl * V + rt;
+		if (rt >= V)
+			return;
+		if (flags & 1)
+			acc = 0.0;
+		const int kn = d.elems / V;
+		#pragma unroll 4
+		for (int k = 0; k < kn; k++)
+			acc = __fma_rn(sv[off + k * V + rt], xg[off + k * V + rt], acc);
+		if (flags & 2) {
+			const int64_t row = (int64_t) d.unit0 * V + rt;
 			if (row < a.m)
 				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
 		}
 	}
+}
+
+// Block-table order of the warp-specialised kernel.  A group is a block of whole units or
+// the full run of chunk blocks of one long unit.  CTA c of G walks groups c, c + G,
+// c + 2G, ... (so, as in a round-robin walk, the CTAs work on neighbouring groups at any
+// moment), and its groups are stored contiguously: the table is permuted once at set-up
+// and CTA c's range is [ranges[c], ranges[c + 1]).
+__device__ __forceinline__ bool ws_group_start(const StagedBlock & d)
+{
+	return d.units >= 0 || ((-d.units - 1) & 1);
+}
+
+__device__ __forceinline__ int64_t ws_group_rank(int64_t g, int64_t G, int64_t q, int64_t rem)
+{
+	const int64_t c = g % G;
+	return c * q + (c < rem ? c : rem) + g / G;
+}
+
+__global__ void ws_group_flag_kernel(const StagedBlock * blocks, int64_t nb, int64_t * flag)
+{
+	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (b < nb)
+		flag[b] = ws_group_start(blocks[b]) ? 1 : 0;
+}
+
+__global__ void ws_group_start_kernel(const StagedBlock * blocks, int64_t nb, const int64_t * pos, int64_t * gs)
+{
+	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (b < nb && ws_group_start(blocks[b]))
+		gs[pos[b]] = b;
+	if (b == 0)
+		gs[pos[nb]] = nb;
+}
+
+__global__ void ws_group_size_kernel(const int64_t * gs, int64_t ng, int64_t G, int64_t * size_by_rank)
+{
+	const int64_t g = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (g < ng)
+		size_by_rank[ws_group_rank(g, G, ng / G, ng % G)] = gs[g + 1] - gs[g];
+}
+
+__global__ void ws_permute_kernel(const StagedBlock * in, int64_t nb, const int64_t * pos, const int64_t * gs,
+		const int64_t * off_by_rank, int64_t ng, int64_t G, StagedBlock * out)
+{
+	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (b >= nb)
+		return;
+	const StagedBlock d = in[b];
+	const int64_t g = pos[b] + (ws_group_start(d) ? 1 : 0) - 1;
+	out[off_by_rank[ws_group_rank(g, G, ng / G, ng % G)] + (b - gs[g])] = d;
+}
+
+__global__ void ws_ranges_kernel(const int64_t * off_by_rank, int64_t ng, int64_t G, int64_t * ranges)
+{
+	const int64_t c = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (c > G)
+		return;
+	const int64_t q = ng / G, rem = ng % G;
+	int64_t r = c * q + (c < rem ? c : rem);
+	ranges[c] = off_by_rank[r < ng ? r : ng];
 }
 
 template <Kind K, Arith A, int L, bool YMAP>
@@ -736,16 +793,17 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 	__syncthreads();
 	int s = 0;
 	uint32_t parity = 0;
+	const int64_t b_begin = a.ranges[blockIdx.x], b_end = a.ranges[blockIdx.x + 1];
 	if ((int) threadIdx.x < ng) {
 		// ---- gather warps
 		const int gt = threadIdx.x;
-		for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+		for (int64_t b = b_begin; b < b_end; b++) {
 			if (!mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles)) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 				return;
 			}
 			const StagedBlock d = sdesc[s];
-			if (d.units >= 0) {
+			if (d.elems > 0) {
 				uint8_t * st = smem + (size_t) s * a.stage_bytes;
 				double * sv = reinterpret_cast<double *>(st);
 				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cap_al * 8);
@@ -785,18 +843,23 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 	const int rt = (int) threadIdx.x - ng;
 	if (rt == 0)
 		for (int q = 0; q < S; q++) {
-			const int64_t b = (int64_t) blockIdx.x + (int64_t) q * gridDim.x;
-			if (b < a.nblocks) {
+			const int64_t b = b_begin + q;
+			if (b < b_end) {
 				const StagedBlock d = a.blocks[b];
 				sdesc[q] = d;
-				staged_issue_d(a, d, q, smem, full);
+				ws_issue(a, d, q, smem, full);
 			}
 		}
 	named_bar_sync(1, nr);
-	for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
-		const int64_t nb = b + (int64_t) S * gridDim.x;
+	double acc = 0.0;          // running state of a long unit across its chunk blocks
+	double ln[L];
+	#pragma unroll
+	for (int l = 0; l < L; l++)
+		ln[l] = 0.0;
+	for (int64_t b = b_begin; b < b_end; b++) {
+		const int64_t nb = b + S;
 		StagedBlock dnext{};
-		if (rt == 0 && nb < a.nblocks)
+		if (rt == 0 && nb < b_end)
 			dnext = a.blocks[nb];
 		const StagedBlock d = sdesc[s];
 		int js0 = 0, je0 = 0;
@@ -812,11 +875,12 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 			rows_t<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(st),
 					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), js0, je0, rt, nr);
 		else
-			ws_long_unit<K, A, L, YMAP>(a, d, reinterpret_cast<double *>(st), rt, nr);
+			ws_chunk<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(st),
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), rt, acc, ln);
 		named_bar_sync(1, nr);
-		if (rt == 0 && nb < a.nblocks) {
+		if (rt == 0 && nb < b_end) {
 			sdesc[s] = dnext;
-			staged_issue_d(a, dnext, s, smem, full);
+			ws_issue(a, dnext, s, smem, full);
 		}
 		if (++s == S) {
 			s = 0;
@@ -1071,6 +1135,44 @@ int batch_occupancy(int threads, size_t smem, int * per_sm)
 	return SPMV_OK;
 }
 
+// Permutes the block table into the warp-specialised kernel's per-CTA group order and
+// writes each CTA's range (h.grid CTAs).
+int ws_order_blocks(Handle & h)
+{
+	cudaStream_t s = h.stream;
+	const int64_t nb = h.num_blocks, G = h.grid;
+	SPMV_TRY(h.alloc(&h.d_cta_ranges, G + 1));
+	DevBuf flag, pos, gs, sz, off, tmp;
+	SPMV_TRY(flag.alloc((nb + 1) * sizeof(int64_t), s));
+	SPMV_TRY(pos.alloc((nb + 1) * sizeof(int64_t), s));
+	const unsigned gb = (unsigned) ceil_div(nb > 0 ? nb : 1, 256);
+	ws_group_flag_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, flag.as<int64_t>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	SPMV_TRY(scan_exclusive(flag.as<int64_t>(), pos.as<int64_t>(), nb, s));
+	int64_t ng = 0;
+	SPMV_CUDA_TRY(cudaMemcpyAsync(&ng, pos.as<int64_t>() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	SPMV_TRY(gs.alloc((ng + 1) * sizeof(int64_t), s));
+	SPMV_TRY(sz.alloc((ng + 1) * sizeof(int64_t), s));
+	SPMV_TRY(off.alloc((ng + 1) * sizeof(int64_t), s));
+	SPMV_TRY(tmp.alloc((nb + 1) * sizeof(StagedBlock), s));
+	ws_group_start_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, pos.as<int64_t>(), gs.as<int64_t>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	if (ng > 0) {
+		ws_group_size_kernel<<<(unsigned) ceil_div(ng, 256), 256, 0, s>>>(gs.as<int64_t>(), ng, G, sz.as<int64_t>());
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	SPMV_TRY(scan_exclusive(sz.as<int64_t>(), off.as<int64_t>(), ng, s));
+	ws_permute_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, pos.as<int64_t>(), gs.as<int64_t>(), off.as<int64_t>(), ng, G,
+			tmp.as<StagedBlock>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	if (nb > 0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_blocks, tmp.p, nb * sizeof(StagedBlock), cudaMemcpyDeviceToDevice, s));
+	ws_ranges_kernel<<<(unsigned) ceil_div(G + 1, 256), 256, 0, s>>>(off.as<int64_t>(), ng, G, h.d_cta_ranges);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	return SPMV_OK;
+}
+
 // Grid / shared-memory geometry of the staged kernel for this handle.
 int staged_geometry(Handle & h)
 {
@@ -1105,7 +1207,7 @@ int staged_geometry(Handle & h)
 		if (g > h.num_blocks)
 			g = h.num_blocks;
 		h.grid = (int) (g > 0 ? g : 1);
-		return SPMV_OK;
+		return ws_order_blocks(h);
 	}
 	if (h.exec_kernel == 3) {
 		const int cap_al = h.block_cap + 8;
@@ -1258,6 +1360,7 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		kern = pick_ws(h);
 		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
 		a.row_threads = h.row_threads;
+		a.ranges = h.d_cta_ranges;
 	}
 	kern<<<h.grid, h.threads, h.smem_bytes, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
