@@ -96,6 +96,28 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t * bar, uint32_t parit
 	return true;
 }
 
+// Named barrier over n threads (a multiple of 32) of the CTA.
+__device__ __forceinline__ void named_bar_sync(int id, int n)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Named barrier over n threads that also returns whether any of them passed `pred` true
+// (so a decision to leave is taken by all of them together).
+__device__ __forceinline__ bool named_bar_or(int id, int n, bool pred)
+{
+	uint32_t out;
+	asm volatile(
+	    "{\n\t.reg .pred p, q;\n\t"
+	    "setp.ne.u32 p, %1, 0;\n\t"
+	    "bar.red.or.pred q, %2, %3, p;\n\t"
+	    "selp.u32 %0, 1, 0, q;\n\t}"
+	    : "=r"(out)
+	    : "r"((uint32_t) pred), "r"(id), "r"(n)
+	    : "memory");
+	return out != 0;
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem()
 {
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -124,6 +146,9 @@ __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b)
 {
 	return (a + b - 1) / b;
 }
+
+// x loads a gather thread of the warp-specialised kernels keeps in flight per round.
+static constexpr int WS_GATHER_SLOTS = 4;
 
 static constexpr long long kWaitBudgetCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 

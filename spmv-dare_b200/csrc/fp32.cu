@@ -172,6 +172,169 @@ __global__ void __launch_bounds__(F32_THREADS) f32_kernel(F32Args a)
 	}
 }
 
+// ------------------------------------------------------------------ warp-specialised FP32 kernel
+// The FP64 warp-specialised kernel's structure (spmv_kernels.cu: gather warps fetch x for
+// block k+1 while row warps sum block k; long rows as chunk runs in per-CTA group order)
+// with FP32 entries: the stage holds values (4 B) | columns (4 B) | gathered x (4 B).
+// Every row, long ones included, is one sequential Dot2 chain.
+struct F32WsArgs {
+	const StagedBlock * blocks;
+	const int64_t * ranges;
+	const int32_t * rp;
+	const int32_t * cols;
+	const float * vals;
+	const float * x;
+	float * y;
+	int cap_al;
+	int stages;
+	int stage_bytes;
+	int row_threads;
+	int * err;
+};
+
+__device__ __forceinline__ void f32ws_issue(const F32WsArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
+{
+	if (d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	float * sv = reinterpret_cast<float *>(smem + (size_t) s * a.stage_bytes);
+	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 4);
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 8u);
+	bulk_g2s(sv, a.vals + e0, cnt * 4u, &bars[s]);
+	bulk_g2s(sc, a.cols + e0, cnt * 4u, &bars[s]);
+}
+
+__global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	__shared__ StagedBlock sdesc[8];
+	const int S = a.stages;
+	uint64_t * full = reinterpret_cast<uint64_t *>(smem + (size_t) S * a.stage_bytes);
+	uint64_t * prod = full + S;
+	const int nr = a.row_threads;
+	const int ng = (int) blockDim.x - nr;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < S; s++) {
+			mbar_init(&full[s], 1);
+			mbar_init(&prod[s], (uint32_t) ng);
+		}
+		mbar_fence_init();
+	}
+	__syncthreads();
+	int s = 0;
+	uint32_t parity = 0;
+	const int64_t b_begin = a.ranges[blockIdx.x], b_end = a.ranges[blockIdx.x + 1];
+	if ((int) threadIdx.x < ng) {
+		// ---- gather warps: x of every staged entry, WS_GATHER_SLOTS loads in flight per thread
+		const int gt = threadIdx.x;
+		for (int64_t b = b_begin; b < b_end; b++) {
+			if (!mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles)) {
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				return;
+			}
+			const StagedBlock d = sdesc[s];
+			if (d.elems > 0) {
+				uint8_t * st = smem + (size_t) s * a.stage_bytes;
+				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cap_al * 4);
+				float * xg = reinterpret_cast<float *>(st + (size_t) a.cap_al * 8);
+				const int off = d.elem0 & 3;
+				for (int e0 = gt; e0 < d.elems; e0 += WS_GATHER_SLOTS * ng) {
+					float xv[WS_GATHER_SLOTS];
+					#pragma unroll
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
+						const int e = e0 + k * ng;
+						if (e < d.elems)
+							xv[k] = __ldg(a.x + sc[off + e]);
+					}
+					#pragma unroll
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
+						const int e = e0 + k * ng;
+						if (e < d.elems)
+							xg[off + e] = xv[k];
+					}
+				}
+			}
+			mbar_arrive(&prod[s]);
+			if (++s == S) {
+				s = 0;
+				parity ^= 1u;
+			}
+		}
+		return;
+	}
+	// ---- row warps
+	const int rt = (int) threadIdx.x - ng;
+	if (rt == 0)
+		for (int q = 0; q < S; q++) {
+			const int64_t b = b_begin + q;
+			if (b < b_end) {
+				const StagedBlock d = a.blocks[b];
+				sdesc[q] = d;
+				f32ws_issue(a, d, q, smem, full);
+			}
+		}
+	named_bar_sync(1, nr);
+	float ls = 0.0f, lc = 0.0f;      // running Dot2 pair of a long row across its chunks
+	for (int64_t b = b_begin; b < b_end; b++) {
+		const int64_t nb = b + S;
+		StagedBlock dnext{};
+		if (rt == 0 && nb < b_end)
+			dnext = a.blocks[nb];
+		const StagedBlock d = sdesc[s];
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		int js = 0, je = 0;
+		if (d.units >= 0 && rt < d.units) {
+			const int64_t r = (int64_t) d.unit0 + rt;
+			js = (int) ((int64_t) __ldg(a.rp + r) - e0);
+			je = (int) ((int64_t) __ldg(a.rp + r + 1) - e0);
+		}
+		const bool ok = mbar_wait_bounded(&prod[s], parity, kWaitBudgetCycles);
+		if (named_bar_or(1, nr, !ok)) {      // all row threads leave together
+			if (rt == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		const uint8_t * st = smem + (size_t) s * a.stage_bytes;
+		const float * sv = reinterpret_cast<const float *>(st);
+		const float * xg = reinterpret_cast<const float *>(st + (size_t) a.cap_al * 8);
+		if (d.units >= 0) {
+			if (rt < d.units) {
+				float sum = 0.0f, c = 0.0f;
+				#pragma unroll 4
+				for (int j = js; j < je; j++)
+					dot2_step(sv[j], xg[j], sum, c);
+				a.y[(int64_t) d.unit0 + rt] = __fadd_rn(sum, c);
+			}
+		} else if (rt == 0) {
+			const int flags = -d.units - 1;
+			const int off = d.elem0 & 3;
+			if (flags & 1) {
+				ls = 0.0f;
+				lc = 0.0f;
+			}
+			#pragma unroll 4
+			for (int e = 0; e < d.elems; e++)
+				dot2_step(sv[off + e], xg[off + e], ls, lc);
+			if (flags & 2)
+				a.y[d.unit0] = __fadd_rn(ls, lc);
+		}
+		named_bar_sync(1, nr);
+		if (rt == 0 && nb < b_end) {
+			sdesc[s] = dnext;
+			f32ws_issue(a, dnext, s, smem, full);
+		}
+		if (++s == S) {
+			s = 0;
+			parity ^= 1u;
+		}
+	}
+}
+
 __global__ void f64_to_f32_kernel(const double * in, float * out, int64_t n)
 {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -195,8 +358,14 @@ __global__ void conv_kernel_f2d(const float * in, double * out, int64_t n)
 
 }  // namespace
 
-// Rounds the stored FP64 values to FP32 and builds the staged block table
-// (blocks of up to 2048 entries by default: 8 bytes per entry staged).
+const void * ws_f32_kernel_fn()
+{
+	return (const void *) ws_f32_kernel;
+}
+
+// Rounds the stored FP64 values to FP32 and builds the staged block table: by default
+// (kernel -1 or 4) the warp-specialised kernel's chunk-run table in per-CTA group order;
+// kernel 0 keeps the CTA staged kernel (blocks of up to 2048 entries, 8 bytes staged each).
 int convert_f32(Handle & h)
 {
 	cudaStream_t s = h.stream;
@@ -205,6 +374,16 @@ int convert_f32(Handle & h)
 	if (h.nnz > 0) {
 		f64_to_f32_kernel<<<(unsigned) ceil_div(h.nnz, 256), 256, 0, s>>>(h.d_v, h.d_vf, h.nnz);
 		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	if (h.desc.kernel < 0 || h.desc.kernel == 4) {
+		spmv_format_desc saved = h.desc;
+		h.desc.kernel = 4;
+		const int st = build_exec(h, h.d_rp, h.m, 1);     // geometry of ws_f32_kernel (values F32)
+		h.desc = saved;
+		if (st != SPMV_OK)
+			return st;
+		h.kernels_per_run = h.num_blocks > 0 ? 1 : 0;
+		return SPMV_OK;
 	}
 	spmv_format_desc saved = h.desc;
 	if (h.desc.block_nnz == 0)
@@ -238,6 +417,24 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 {
 	if (h.num_blocks == 0)
 		return SPMV_OK;
+	if (h.exec_kernel == 4) {
+		F32WsArgs w{};
+		w.blocks = h.d_blocks;
+		w.ranges = h.d_cta_ranges;
+		w.rp = h.d_rp;
+		w.cols = h.d_ci;
+		w.vals = h.d_vf;
+		w.x = d_x;
+		w.y = d_y;
+		w.cap_al = h.block_cap + 8;
+		w.stages = h.stages;
+		w.stage_bytes = (int) (ceil_div((int64_t) w.cap_al * 12, 128) * 128);
+		w.row_threads = h.row_threads;
+		w.err = h.d_err;
+		ws_f32_kernel<<<h.grid, h.threads, h.smem_bytes, s>>>(w);
+		SPMV_CUDA_TRY(cudaGetLastError());
+		return SPMV_OK;
+	}
 	F32Args a{};
 	a.blocks = h.d_blocks;
 	a.nblocks = h.num_blocks;

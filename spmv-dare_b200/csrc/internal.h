@@ -171,6 +171,7 @@ int convert_sell(Handle & h, bool sorted);
 int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
 int convert_f32(Handle & h);
+const void * ws_f32_kernel_fn();   // the FP32 warp-specialised kernel (geometry queries)
 int run_mixed_noalloc(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
 int convert_vector_d2f(const double * in, float * out, int64_t n, cudaStream_t s);
 int convert_vector_f2d(const float * in, double * out, int64_t n, cudaStream_t s);

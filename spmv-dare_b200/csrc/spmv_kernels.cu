@@ -605,27 +605,6 @@ __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock &
 // and their first thread issues the stage's next copy.  Same per-row operation order as
 // staged_kernel; a block holds at most `row_threads` rows, and a unit longer than a block
 // is a run of chunk blocks.  Each CTA walks a contiguous range of the block table.
-__device__ __forceinline__ void named_bar_sync(int id, int n)
-{
-	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-
-// Named barrier over n threads that also returns whether any of them passed `pred` true
-// (so a decision to leave is taken by all of them together).
-__device__ __forceinline__ bool named_bar_or(int id, int n, bool pred)
-{
-	uint32_t out;
-	asm volatile(
-	    "{\n\t.reg .pred p, q;\n\t"
-	    "setp.ne.u32 p, %1, 0;\n\t"
-	    "bar.red.or.pred q, %2, %3, p;\n\t"
-	    "selp.u32 %0, 1, 0, q;\n\t}"
-	    : "=r"(out)
-	    : "r"((uint32_t) pred), "r"(id), "r"(n)
-	    : "memory");
-	return out != 0;
-}
-
 // Bulk copy of a block's entries for the warp-specialised kernel (chunk blocks of long
 // units included; only an empty block completes the stage without a copy).
 __device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
@@ -809,18 +788,18 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cap_al * 8);
 				double * xg = reinterpret_cast<double *>(st + (size_t) a.cap_al * 12);
 				const int off = d.elem0 & 3;
-				// 4 independent loads in flight per thread: the column loads of a group are
+				// WS_GATHER_SLOTS independent loads in flight per thread: the column loads of a group are
 				// all issued before any store of the group, so the x loads overlap
-				for (int e0 = gt; e0 < d.elems; e0 += 4 * ng) {
-					double xv[4];
+				for (int e0 = gt; e0 < d.elems; e0 += WS_GATHER_SLOTS * ng) {
+					double xv[WS_GATHER_SLOTS];
 					#pragma unroll
-					for (int k = 0; k < 4; k++) {
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
 						const int e = e0 + k * ng;
 						if (e < d.elems)
 							xv[k] = ldg(a.x + sc[off + e]);
 					}
 					#pragma unroll
-					for (int k = 0; k < 4; k++) {
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
 						const int e = e0 + k * ng;
 						if (e < d.elems) {
 							if (A == Arith::SEQ_SPLIT)
@@ -1190,7 +1169,8 @@ int staged_geometry(Handle & h)
 		if (h.stages < 2)
 			h.stages = 2;
 		h.smem_bytes = (size_t) h.stages * stage_bytes + (size_t) h.stages * 16;
-		StagedFn kern = pick_ws(h);
+		// FP32-value handles run ws_f32_kernel (fp32.cu), whose stage is also 12 B per entry
+		const void * kern = (h.desc.values == SPMV_VALUES_F32) ? ws_f32_kernel_fn() : (const void *) pick_ws(h);
 		if (!kern) {
 			set_error(SPMV_ERR_ARG, "no warp-specialised kernel for format %d with vec_len %d", h.desc.format,
 					h.desc.vec_len);
