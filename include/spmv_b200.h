@@ -178,6 +178,43 @@ int spmv_run_f32(spmv_handle * h, const float * x, float * y);
 #define SPMV_NOALLOC_MAX_ELEMS 262144
 int spmv_run_device_mixed_noalloc(spmv_handle * h, const double * d_x, double * d_y, void * stream);
 
+/* ------------------------------------------------------------------ learned selector
+ * No counterpart in the reference's SpMV path: its generator computes the same statistics on
+ * the host (artificial-matrix-generator/artificial_matrix_generation.c:529-570, matrix_util.h).
+ *
+ * spmv_features(_device): the 10 structural features of a CSR matrix, computed on the GPU:
+ *   [0] log2(m+1)  [1] log2(nnz+1)  [2] avg nnz/row  [3] std/avg nnz/row  [4] skew (max-avg)/avg
+ *   [5] mean row bandwidth / n  [6] mean row scatter (degree / bandwidth)
+ *   [7] avg neighbours (2 x entries within +1 column after each entry, per nnz)
+ *   [8] cross-row similarity with the next non-empty row (window 1)
+ *   [9] mean groups of consecutive columns / degree
+ * Host arrays (copied) or device arrays on `stream`; out10 is host memory.
+ */
+int spmv_features(const int32_t * row_ptr, const int32_t * col_ind, int64_t m, int64_t n, int64_t nnz, double * out10);
+int spmv_features_device(const int32_t * d_row_ptr, const int32_t * d_col_ind, int64_t m, int64_t n, int64_t nnz,
+		double * out10, void * stream);
+
+/* FP32 MLP in -> h1 -> h2 -> out (ReLU hidden layers, softmax cross-entropy on the logits),
+ * trained and run by hand-written kernels.  Parameters are contiguous: W1[h1][in], b1[h1],
+ * W2[h2][h1], b2[h2], W3[out][h2], b3[out] (spmv_mlp_num_params floats); init_params gives
+ * their initial values (host).  spmv_mlp_get copies (0) parameters, (1) gradients of the
+ * last spmv_mlp_loss_grad, (2) / (3) Adam first / second moments to host; spmv_mlp_set loads
+ * parameters.  Batches are row-major [batch][in] device arrays; labels int32 class indices;
+ * spmv_mlp_loss_grad writes the batch-mean loss to *loss_out (host) when given. */
+typedef struct spmv_mlp spmv_mlp;
+spmv_mlp * spmv_mlp_create(int32_t in, int32_t h1, int32_t h2, int32_t out, const float * init_params, int * status);
+int32_t spmv_mlp_num_params(const spmv_mlp * mlp);
+int spmv_mlp_get(const spmv_mlp * mlp, int32_t which, float * host_out);
+int spmv_mlp_set(spmv_mlp * mlp, const float * host_params);
+int spmv_mlp_forward(spmv_mlp * mlp, const float * d_x, int32_t batch, float * d_logits, void * stream);
+/* Host-buffer inference: copies [batch][in] inputs in, runs the forward pass, copies the
+ * [batch][out] logits back and waits (the selector's per-matrix query). */
+int spmv_mlp_forward_host(spmv_mlp * mlp, const float * x_host, int32_t batch, float * logits_host);
+int spmv_mlp_loss_grad(spmv_mlp * mlp, const float * d_x, const int32_t * d_labels, int32_t batch, float * loss_out,
+		void * stream);
+int spmv_mlp_adam_step(spmv_mlp * mlp, float lr, float beta1, float beta2, float eps, float weight_decay, void * stream);
+void spmv_mlp_destroy(spmv_mlp * mlp);
+
 /* Waits for the handle's stream and returns the first device-side error, if any. */
 int spmv_sync(spmv_handle * h);
 

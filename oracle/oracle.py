@@ -300,6 +300,8 @@ def _ref(name):
             L.ref_gen_stats.argtypes = [c_void_p, c_void_p]
             L.ref_gen_num_stats.restype = c_int
             L.ref_gen_free.argtypes = [c_void_p]
+            L.ref_cross_row_similarity.restype = c_double
+            L.ref_cross_row_similarity.argtypes = [c_void_p, c_void_p, c_long, c_long, c_long, c_int]
         elif name == "sellcs":
             L.ref_sellcs_convert.restype = c_void_p
             L.ref_sellcs_convert.argtypes = [c_void_p] * 3 + [c_long] * 5
@@ -354,6 +356,12 @@ def ref_generate(rows, cols, avg, std, distribution, placement, bw, skew, neigh,
     finally:
         L.ref_gen_free(h)
     return rp, ci[:nnz], v[:nnz], dict(zip(STAT_NAMES, st.tolist()))
+
+
+def ref_cross_row_similarity(rp, ci, n, threads=8):
+    """The reference's csr_cross_row_similarity (matrix_util.h:269-328), window 1."""
+    rp, ci = _c(rp, np.int32), _c(ci, np.int32)
+    return _ref("gen").ref_cross_row_similarity(_p(rp), _p(ci), rp.size - 1, n, int(rp[-1]), threads)
 
 
 class RefFormat:
@@ -429,3 +437,99 @@ def ref_sellcs_convert(rp, ci, v, C, sigma):
         L.ref_sellcs_free(h)
     return dict(row_order=ro[:m], slice_widths=w[:ns], slice_pointers=ptr, column_indices=cols[:size],
                 values=vals[:size])
+
+
+# ------------------------------------------------------------------ learned selector
+def features(rp, ci, m, n):
+    """The 10 structural features in numpy FP64 (the statistics of
+    artificial-matrix-generator/artificial_matrix_generation.c:529-570 and
+    matrix_util.h:206-300 with window 1; cross-row similarity as csr_cross_row_similarity,
+    the mean over non-empty rows)."""
+    rp = np.asarray(rp, np.int64)
+    ci = np.asarray(ci, np.int64)
+    nnz = int(rp[-1]) if m > 0 else 0
+    deg = np.diff(rp).astype(np.float64)
+    md = float(m) if m > 0 else 1.0
+    avg = deg.sum() / md
+    var = (deg * deg).sum() / md - avg * avg
+    ne = deg > 0
+    first = np.where(ne, ci[np.minimum(rp[:-1], max(nnz - 1, 0))] if nnz else 0, 0)
+    last = np.where(ne, ci[np.maximum(rp[1:] - 1, 0)] if nnz else 0, 0)
+    bw = np.where(ne, last - first + 1, 0).astype(np.float64)
+    rows = np.repeat(np.arange(m), np.diff(rp))
+    same = rows[1:] == rows[:-1] if nnz > 1 else np.zeros(0, bool)
+    d = np.diff(ci) if nnz > 1 else np.zeros(0, np.int64)
+    consec = np.bincount(rows[1:][same & (d <= 1)], minlength=m) if nnz > 1 else np.zeros(m)
+    newgrp = np.bincount(rows[1:][same & (d > 1)], minlength=m) if nnz > 1 else np.zeros(m)
+    groups = np.where(ne, 1 + newgrp, 0)
+    # cross-row similarity: each non-empty row against the next non-empty row
+    nz_rows = np.nonzero(ne)[0]
+    crs = 0.0
+    if nz_rows.size > 1:
+        nxt = np.full(m, -1, np.int64)
+        nxt[nz_rows[:-1]] = nz_rows[1:]
+        W = n + 3
+        key = rows * W + ci
+        tgt = nxt[rows]
+        ok = tgt >= 0
+        lo = tgt * W + ci - 1
+        idx = np.searchsorted(key, lo, "left")
+        hit = ok & (idx < nnz)
+        hit[hit] = key[idx[hit]] <= (tgt * W + ci + 1)[hit]
+        sim = np.bincount(rows[hit], minlength=m).astype(np.float64)
+        crs = float(np.sum(np.where(ne, sim / np.maximum(deg, 1), 0.0)))
+    out = np.zeros(10)
+    out[0] = np.log2(m + 1.0)
+    out[1] = np.log2(nnz + 1.0)
+    out[2] = avg
+    out[3] = np.sqrt(max(var, 0.0)) / avg if avg > 0 else 0.0
+    out[4] = (deg.max() - avg) / avg if avg > 0 else 0.0
+    out[5] = (bw / n).sum() / md if n > 0 else 0.0
+    out[6] = np.where(ne, deg / np.maximum(bw, 1), 0.0).sum() / md
+    out[7] = 2.0 * consec.sum() / nnz if nnz > 0 else 0.0
+    out[8] = crs / nz_rows.size if nz_rows.size > 0 else 0.0
+    out[9] = np.where(ne, groups / np.maximum(deg, 1), 0.0).sum() / md
+    return out
+
+
+def mlp_offsets(dims):
+    """Offsets of W1, b1, W2, b2, W3, b3 in the flat parameter vector."""
+    offs, o = [], 0
+    for l in range(3):
+        offs.append((o, o + dims[l + 1] * dims[l]))
+        o += dims[l + 1] * dims[l] + dims[l + 1]
+    return offs, o
+
+
+def mlp_loss_grad(params, dims, X, labels):
+    """FP64 forward + backward of the selector MLP (ReLU hidden layers, mean softmax
+    cross-entropy): (loss, flat gradient, logits)."""
+    p = np.asarray(params, np.float64)
+    offs, total = mlp_offsets(dims)
+    Ws = [p[w0:b0].reshape(dims[l + 1], dims[l]) for l, (w0, b0) in enumerate(offs)]
+    bs = [p[b0:b0 + dims[l + 1]] for l, (w0, b0) in enumerate(offs)]
+    X = np.asarray(X, np.float64)
+    B = X.shape[0]
+    z1 = X @ Ws[0].T + bs[0]
+    a1 = np.maximum(z1, 0)
+    z2 = a1 @ Ws[1].T + bs[1]
+    a2 = np.maximum(z2, 0)
+    z3 = a2 @ Ws[2].T + bs[2]
+    mx = z3.max(1, keepdims=True)
+    lse = mx[:, 0] + np.log(np.exp(z3 - mx).sum(1))
+    y = np.asarray(labels, np.int64)
+    loss = float(np.mean(lse - z3[np.arange(B), y]))
+    d3 = np.exp(z3 - lse[:, None])
+    d3[np.arange(B), y] -= 1.0
+    d3 /= B
+    g = np.zeros(total)
+    acts = [X, a1, a2]
+    zs = [z1, z2]
+    d = d3
+    for l in (2, 1, 0):
+        w0, b0 = offs[l]
+        g[w0:b0] = (d.T @ acts[l]).ravel()
+        g[b0:b0 + dims[l + 1]] = d.sum(0)
+        if l > 0:
+            d = (d @ Ws[l]) * (zs[l - 1] > 0)
+    return loss, g, z3

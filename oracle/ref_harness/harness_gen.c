@@ -62,3 +62,14 @@ EXPORT void ref_gen_free(void * p)
 {
 	free_csr_matrix((struct csr_matrix *) p);
 }
+
+/* The reference's cross-row similarity over non-empty rows (matrix_util.h:269-328, window
+ * 1), called directly: the generator's own value (csr_cross_row_similarity2) averages over
+ * a partly uninitialised buffer, so the selector's feature is pinned on this one. */
+#include "matrix_util.h"
+
+EXPORT double ref_cross_row_similarity(int32_t * row_ptr, int32_t * col, long m, long n, long nnz, int num_threads)
+{
+	omp_set_num_threads(num_threads);
+	return csr_cross_row_similarity((int *) row_ptr, (int *) col, m, n, nnz, 1);
+}

@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_char, c_char_p, c_double, c_int, c_int32, c_int64, c_uint32, c_void_p
+from ctypes import POINTER, c_char, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint32, c_void_p
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "lib", "libspmv_b200.so")
@@ -78,6 +78,17 @@ SIGNATURES = {
     "spmv_run_device_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_run_f32": (c_int, [c_void_p, c_void_p, c_void_p]),
     "spmv_run_device_mixed_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_features": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p]),
+    "spmv_features_device": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p, c_void_p]),
+    "spmv_mlp_create": (c_void_p, [c_int32, c_int32, c_int32, c_int32, c_void_p, POINTER(c_int)]),
+    "spmv_mlp_num_params": (c_int32, [c_void_p]),
+    "spmv_mlp_get": (c_int, [c_void_p, c_int32, c_void_p]),
+    "spmv_mlp_set": (c_int, [c_void_p, c_void_p]),
+    "spmv_mlp_forward": (c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p]),
+    "spmv_mlp_forward_host": (c_int, [c_void_p, c_void_p, c_int32, c_void_p]),
+    "spmv_mlp_loss_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p]),
+    "spmv_mlp_adam_step": (c_int, [c_void_p, c_float, c_float, c_float, c_float, c_float, c_void_p]),
+    "spmv_mlp_destroy": (None, [c_void_p]),
     "spmv_sync": (c_int, [c_void_p]),
     "spmv_get_info": (c_int, [c_void_p, POINTER(Info)]),
     "spmv_export": (c_int, [c_void_p, c_int32, c_void_p, POINTER(c_int64)]),

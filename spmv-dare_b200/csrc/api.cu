@@ -27,7 +27,7 @@ int last_status()
 	return g_status;
 }
 
-static void clear_error()
+void clear_error()
 {
 	g_status = SPMV_OK;
 	g_msg[0] = 0;

@@ -12,6 +12,7 @@ namespace spmv {
 
 // ------------------------------------------------------------------ host error plumbing
 void set_error(int code, const char * fmt, ...);
+void clear_error();
 int  last_status();
 
 #define SPMV_CUDA_TRY(expr)                                                                      \
