@@ -18,6 +18,14 @@ the headline `value` is --format.
 
 --impl reference times the reference's own CPU implementation of the same format, compiled
 from its sources (oracle/_ref), on all host cores.
+
+--workload batch: the batched engine on 512 artificial matrices (seeds 1000-1511, rows
+log-uniform in [1e3, 2e5], parameters from spmv-dare_b200/workloads.py), each in the format
+the exhaustive autotuner picked for it (spmv-dare_b200/data/tune_batch.npz; --retune
+re-runs the autotuner here).  A step is one SpMV of every matrix: one CUDA-graph replay of
+the persistent work-queue kernel (`value`), beside the same batch launched directly and the
+512 matrices launched one by one with their own handles.  Metric: the aggregate algorithmic
+bytes of the 512 SpMVs over the step time.
 """
 from __future__ import annotations
 
@@ -423,6 +431,227 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+BATCH_SEEDS = (1000, 1512)
+BATCH_WORKLOAD = ("batch: 512 artificial matrices, seeds 1000-1511, rows log-uniform [1e3, 2e5], avg U[5,60], "
+                  "std U[0.1,1]xavg, normal/gamma, skew U[0,200], bw U[0.01,0.5], random placement")
+
+
+def batch_matrices(sb, count, retune=False):
+    """(matrices, per-matrix class, x vectors, total bytes) of the batched workload."""
+    pkg = os.path.join(ROOT, "spmv-dare_b200")
+    sys.path.insert(0, pkg)
+    from spmv_dare_b200 import tuning, workloads
+
+    best = {}
+    db_path = os.path.join(pkg, "data", "tune_batch.npz")
+    if not retune and os.path.exists(db_path):
+        with np.load(db_path) as z:
+            best = dict(zip(z["seeds"].tolist(), z["best"].tolist()))
+    timer = None
+    mats, classes, xs, B = [], [], [], 0
+    for seed in range(BATCH_SEEDS[0], BATCH_SEEDS[0] + count):
+        p = workloads.batch_params(seed)
+        rp, ci, v, x = workloads.generate(sb, p)
+        m = n = p["rows"]
+        if seed not in best:
+            import torch
+
+            timer = timer or tuning.Timer(torch, "cuda")
+            _, best[seed], _ = tuning.exhaustive(sb, timer, rp, ci, v, m, n, tuning.BATCHABLE, reps=5)
+        mats.append((rp, ci, v, m, n))
+        classes.append(int(best[seed]))
+        xs.append(x)
+        B += algorithmic_bytes(m, n, int(rp[-1]))
+    return mats, classes, xs, B
+
+
+def time_events(fn, steps, warmup, torch):
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for k in range(steps):
+        fn()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[steps]) / steps, [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+
+
+def run_batch(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    sb = load_package()
+    from spmv_dare_b200 import tuning
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mats, classes, xs, B = batch_matrices(sb, args.batch_count, args.retune)
+    nnz_total = sum(int(mt[0][-1]) for mt in mats)
+    batch = sb.Batch(mats, [tuning.batch_desc(c) for c in classes])
+    xh = np.concatenate(xs)
+    xd = torch.from_numpy(xh).to(dev)
+    yd = torch.empty(batch.total_y, dtype=torch.float64, device=dev)
+    peak, peak_kind = hbm_peak()
+
+    sampler = ClockSampler(local)
+    barrier(world)
+    sampler.start()
+    ms_graph, per = time_events(lambda: batch.spmv(xd, yd, graph=True), args.steps, args.warmup, torch)
+    clocks = sampler.stop()
+    barrier(world)
+    ms_graph = max_over_ranks(world, ms_graph)
+    y_batch = yd.cpu().numpy().copy()
+    ms_direct, _ = time_events(lambda: batch.spmv(xd, yd, graph=False), args.steps, args.warmup, torch)
+
+    # the same matrices one launch each, with their own handles (each class's full tuning)
+    handles = []
+    for (rp, ci, v, m, n), c in zip(mats, classes):
+        handles.append(sb.csr_to_format(rp, ci, v, m, n, int(rp[-1]), **tuning.CLASSES[c]))
+    xo, yo = batch.x_offsets, batch.y_offsets
+    views = [(xd[int(xo[i]):int(xo[i]) + mats[i][4]], yd[int(yo[i]):int(yo[i]) + mats[i][3]]) for i in range(len(mats))]
+
+    def per_matrix():
+        for h, (xv, yv) in zip(handles, views):
+            h.spmv(xv, yv)
+
+    ms_loop, _ = time_events(per_matrix, max(3, args.steps // 5), 3, torch)
+    y_loop = yd.cpu().numpy()
+    identical = bool(np.array_equal(y_batch.view(np.uint64), y_loop.view(np.uint64)))
+    for h in handles:
+        h.destroy()
+
+    # e2e: host x in (pinned), one graph replay, host y out, every step
+    xp = torch.from_numpy(xh).pin_memory()
+    yp = torch.empty(batch.total_y, dtype=torch.float64).pin_memory()
+
+    def e2e():
+        xd.copy_(xp, non_blocking=True)
+        batch.spmv(xd, yd, graph=True)
+        yp.copy_(yd, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
+
+    achieved = B * 1e-9 / (statistics.median(per) * 1e-3)
+    fmt_counts = {}
+    for c in classes:
+        fmt_counts[tuning.class_name(c)] = fmt_counts.get(tuning.class_name(c), 0) + 1
+    out = {
+        "metric": "batched SpMV GB/s (aggregate algorithmic bytes of all matrices / step time)",
+        "value": round(world * B * 1e-9 / (ms_graph * 1e-3), 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_graph, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference's artificial generator restated natively; values 2v-1, x U[-1,1))",
+        "config": {"workload": BATCH_WORKLOAD, "matrices": len(mats), "nnz_total": nnz_total, "bytes_per_step": B,
+                   "formats": fmt_counts, "tuning": "exhaustive autotuner over the batchable classes",
+                   "l2": f"no flush: inputs ({B / 1e9:.2f} GB/step) exceed the 126 MB L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s", "h2d_bytes_per_step": int(xh.nbytes),
+                "d2h_bytes_per_step": int(batch.total_y * 8), "ms_per_step": round(e2e_s * 1e3, 4)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s"},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "batch": {"graph_ms": round(ms_graph, 4), "direct_ms": round(ms_direct, 4), "per_matrix_launches_ms": round(ms_loop, 4),
+                  "graph_gbs": round(B * 1e-9 / (ms_graph * 1e-3), 1), "direct_gbs": round(B * 1e-9 / (ms_direct * 1e-3), 1),
+                  "per_matrix_gbs": round(B * 1e-9 / (ms_loop * 1e-3), 1), "y_identical_to_per_matrix": identical,
+                  "blocks": int(batch.num_blocks)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with stdout_to_stderr():
+            out["cpu_baseline"] = batch_cpu_baseline(mats, xs, args.cpu_seconds)
+    batch.destroy()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def ref_batch_pass(mats, xs, reps, cores):
+    """Seconds of one pass of the reference's csr_naive (compiled from its sources, all host
+    cores) over the matrices: each converted, its SpMV timed `reps` times (mean), freed --
+    the reference holds per-thread state in globals, one converted matrix at a time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    total = 0.0
+    for (rp, ci, v, m, n), x in zip(mats, xs):
+        R = O.RefFormat("csr_naive", rp, ci, v, threads=cores)
+        y = np.ones(m + 64)
+        R.spmv(x, y)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            R.spmv(x, y)
+        total += (time.perf_counter() - t0) / reps
+        R.close()
+    return total
+
+
+def batch_cpu_baseline(mats, xs, sample_s=10.0):
+    """The reference's csr_naive on all host cores, one pass over every batch matrix."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    cores = len(os.sched_getaffinity(0))
+    if not O.ref_available("csr_naive"):
+        return {"value": None, "unit": "GB/s", "cores": cores, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libref_csr_naive.so not built"}
+    B = sum(algorithmic_bytes(m, n, int(rp[-1])) for (rp, ci, v, m, n) in mats)
+    reps = 3
+    t = ref_batch_pass(mats, xs, reps, cores)
+    return {"value": round(B * 1e-9 / t, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+            "format": "csr_naive", "ms_per_pass": round(t * 1e3, 3),
+            "sample": f"all {len(mats)} batch matrices, SpMV time of each = mean of {reps} after 1 warm-up, summed"}
+
+
+def run_reference_batch(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    sb = load_package()
+    with stdout_to_stderr():
+        mats, classes, xs, B = batch_matrices(sb, args.batch_count, retune=False)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if not O.ref_available("csr_naive"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_csr_naive.so missing"}))
+        return
+    cores = len(os.sched_getaffinity(0))
+    with stdout_to_stderr():
+        ref_batch_pass(mats[:2], xs[:2], args.warmup, cores)                 # warm-up
+        t = ref_batch_pass(mats, xs, args.steps, cores)
+    per = [t]
+    ms = 1e3 * sum(per) / len(per)
+    val = B * 1e-9 / (ms * 1e-3)
+    print(json.dumps({
+        "metric": "batched SpMV GB/s (aggregate algorithmic bytes of all matrices / step time)",
+        "value": round(val, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference's artificial generator restated natively; values 2v-1, x U[-1,1))",
+        "config": {"workload": BATCH_WORKLOAD, "matrices": len(mats), "bytes_per_step": B, "format": "csr_naive"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                         "sample": f"all {len(mats)} matrices per step; each matrix converted, its SpMV timed "
+                                   f"{args.steps} times (mean), freed; step = sum over matrices"},
+        "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,10 +664,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--rows", type=int, default=0, help="config 2 with this many rows/cols (profiling)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "batch"])
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--retune", action="store_true", help="batch: re-run the autotuner instead of its database")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "batch":
+        (run_reference_batch if args.impl == "reference" else run_batch)(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

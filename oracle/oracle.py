@@ -315,6 +315,7 @@ def _ref(name):
             L.ref_convert.restype = c_void_p
             L.ref_convert.argtypes = [c_void_p] * 3 + [c_long] * 3 + [c_int]
             L.ref_spmv.argtypes = [c_void_p] * 3
+            L.ref_free.argtypes = [c_void_p]
             L.ref_mem_footprint.restype = c_double
             L.ref_mem_footprint.argtypes = [c_void_p]
             L.ref_format_name.restype = c_char_p
@@ -365,7 +366,10 @@ def ref_cross_row_similarity(rp, ci, n, threads=8):
 
 
 class RefFormat:
-    """One reference format compiled from its sources (csr_naive, csr_vec, sell, sell_sorted, div_rf)."""
+    """One reference format compiled from its sources (csr_naive, csr_vec, sell, sell_sorted, div_rf).
+
+    The reference keeps per-thread state of a converted matrix in file-scope globals, so at
+    most one RefFormat of a format may be alive: close() it before converting another."""
 
     def __init__(self, fmt, rp, ci, v, n=None, threads=8):
         self.L = _ref(fmt)
@@ -383,6 +387,11 @@ class RefFormat:
             y = np.ones(self.m + 64, np.float64)
         self.L.ref_spmv(self.h, _p(x), _p(y))
         return y
+
+    def close(self):
+        if self.h:
+            self.L.ref_free(self.h)
+            self.h = None
 
     @property
     def mem_footprint(self):

@@ -67,6 +67,14 @@ EXPORT void ref_spmv(void * mf, double * x, double * y)
 	((struct Matrix_Format *) mf)->spmv(x, y);
 }
 
+/* Destroys a converted matrix.  The reference's formats keep per-thread state in file-scope
+ * globals (e.g. thread_i_s / thread_i_e, src/spmv_kernels/csr.cpp:21-22), so only one
+ * converted matrix may be alive at a time: free it before converting the next. */
+EXPORT void ref_free(void * mf)
+{
+	delete (struct Matrix_Format *) mf;
+}
+
 EXPORT double ref_mem_footprint(void * mf)
 {
 	return ((struct Matrix_Format *) mf)->mem_footprint;
