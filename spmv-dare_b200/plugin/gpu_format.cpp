@@ -105,7 +105,7 @@ csr_to_format(INT_T * row_ptr, INT_T * col_ind, ValueTypeReference * values, lon
 	d.block_nnz = (int32_t) env_long("SPMV_GPU_BLOCK_NNZ", 0);
 	d.stages = (int32_t) env_long("SPMV_GPU_STAGES", 0);
 	d.threads = (int32_t) env_long("SPMV_GPU_THREADS", 0);
-	d.kernel = (int32_t) env_long("SPMV_GPU_KERNEL", 0);
+	d.kernel = (int32_t) env_long("SPMV_GPU_KERNEL", d.kernel);
 #if DOUBLE == 0
 	d.values = SPMV_VALUES_F32;
 #endif

@@ -1,8 +1,9 @@
 """FP32 storage variant (FP32 values, exact int32 indices, Dot2-compensated FP32 rows).
 
-Bars: y bit-identical to the oracle's sequential Dot2 rows (rows that fit one staged
-block; longer rows use a compensated tree and are checked by tolerance), and max relative
-error against the FP64 result <= 1e-6 per row, relative to max(|y_i|, sum_j |a_ij x_j|).
+Bars: y bit-identical to the oracle's sequential Dot2 rows (every row with the default
+warp-specialised kernel; with kernel 0, rows that fit one staged block, longer rows being
+reduced by a compensated tree and checked by tolerance), and max relative error against
+the FP64 result <= 1e-6 per row, relative to max(|y_i|, sum_j |a_ij x_j|).
 """
 import numpy as np
 import pytest
