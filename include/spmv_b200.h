@@ -78,7 +78,8 @@ extern "C" {
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
  *                    threads per CTA), 0 = default.
- *   kernel          -1: the format's default (4 for csr_naive, 0 otherwise);
+ *   kernel          -1: the format's default (4 for csr_naive, 6 for SELL-C-sigma with
+ *                       C <= 32, 0 otherwise);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
  *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);
@@ -86,7 +87,11 @@ extern "C" {
  *                       rows (every format but DIV-RF; block_nnz <= 8 * threads);
  *                    4: warp-specialised staged kernel: gather warps and block_rows row
  *                       threads (default 64 of 160) work on consecutive blocks at once
- *                       (every format but DIV-RF).  default -1
+ *                       (every format but DIV-RF);
+ *                    5: CTA staged kernel whose row threads load their own x, no gather
+ *                       phase (every format but DIV-RF);
+ *                    6: warp-autonomous kernel whose slice rows load their own x, no x
+ *                       buffer (sell, sell_sorted, SELL-C-sigma with C <= 32).  default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;

@@ -421,23 +421,34 @@ int validate_csr(Handle & h)
 }
 
 // Kernel choice: -1 = the format's default (the warp-specialised kernel for csr_naive, the
-// CTA staged kernel otherwise, the fastest of each on the 4M-row configuration); 0 = CTA
+// warp-autonomous own-gather kernel for SELL-C-sigma with C <= 32, the CTA staged kernel
+// otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
 // staged kernel; 1 = direct column-major kernel (slices of >= 32 rows only); 2 =
 // warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
-// block's gather overlapping this block's rows; 4 = warp-specialised staged kernel.
+// block's gather overlapping this block's rows; 4 = warp-specialised staged kernel; 5 = CTA
+// staged kernel whose row threads load their own x (no separate gather phase); 6 =
+// warp-autonomous kernel whose slice rows load their own x (slices of <= 32 rows).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
-	if (k < 0)
-		k = (h.desc.format == SPMV_FMT_CSR_NAIVE) ? 4 : 0;
+	if (k < 0) {
+		if (h.desc.format == SPMV_FMT_CSR_NAIVE)
+			k = 4;
+		else if (h.desc.format == SPMV_FMT_SELL_C_S && V <= 32)
+			k = 6;
+		else
+			k = 0;
+	}
 	if (k == 1 && V < 32)
 		k = 0;
-	if (k == 2 && V > 32)
+	if ((k == 2 || k == 6) && V > 32)
 		k = 0;
+	if (k == 6 && V == 1)
+		k = 2;                      // CSR: the warp kernel's own path
 	h.exec_kernel = k;
 	if (k == 1)
 		return SPMV_OK;
-	if (k == 2)
+	if (k == 2 || k == 6)
 		return build_warp_chunks(h, d_P, U, V);
 	staged_defaults(h);
 	if ((k == 3 || k == 4) && h.desc.stages == 0)

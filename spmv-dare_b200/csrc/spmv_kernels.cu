@@ -296,12 +296,83 @@ __device__ __forceinline__ void block_rows(const StagedArgs & a, const StagedBlo
 	}
 }
 
+// Rows of one staged block, each row thread loading its own x entries (8 independent loads
+// in flight) straight from the staged columns: no CTA-wide gather phase and no barrier
+// between gather and rows.  Same per-row operation order as block_rows.
+template <Kind K, Arith A, int L, bool YMAP>
+__device__ __forceinline__ void own_rows(const StagedArgs & a, const StagedBlock & d, const double * sv, const int32_t * sc,
+		int js0, int je0)
+{
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const double * __restrict__ x = a.x;
+	if (K == Kind::CSR) {
+		for (int u = threadIdx.x; u < d.units; u += blockDim.x) {
+			const int64_t r = (int64_t) d.unit0 + u;
+			const int js = (u == (int) threadIdx.x) ? js0 : (int) ((int64_t) a.ptr[r] - e0);
+			const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
+			double sum = 0.0;
+			if (A == Arith::SEQ_SPLIT) {
+				#pragma unroll 8
+				for (int j = js; j < je; j++)
+					sum = __dadd_rn(sum, __dmul_rn(sv[j], ldg(x + sc[j])));
+			} else if (A == Arith::SEQ_FMA) {
+				#pragma unroll 8
+				for (int j = js; j < je; j++)
+					sum = __fma_rn(sv[j], ldg(x + sc[j]), sum);
+			} else {
+				double ln[L];
+				#pragma unroll
+				for (int l = 0; l < L; l++)
+					ln[l] = 0.0;
+				const int jv = js + ((je - js) & ~(L - 1));
+				#pragma unroll 2
+				for (int j = js; j < jv; j += L) {
+					#pragma unroll
+					for (int l = 0; l < L; l++)
+						ln[l] = __fma_rn(sv[j + l], ldg(x + sc[j + l]), ln[l]);
+				}
+				sum = lanes_reduce<L>(ln);
+				for (int j = jv; j < je; j++)
+					sum = __dadd_rn(sum, __dmul_rn(sv[j], ldg(x + sc[j])));
+			}
+			a.y[r] = sum;
+		}
+	} else {
+		const int V = a.V;
+		const int nrow = d.units * V;
+		for (int u = threadIdx.x; u < nrow; u += blockDim.x) {
+			const int64_t sl = (int64_t) d.unit0 + u / V;
+			const int lane = u % V;
+			const int64_t row = sl * V + lane;
+			if (row >= a.m)
+				continue;
+			const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
+			const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+			double acc = 0.0;
+			#pragma unroll 8
+			for (int k = 0; k < w; k++)
+				acc = __fma_rn(sv[ks + k * V], ldg(x + sc[ks + k * V]), acc);
+			a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+		}
+	}
+}
+
 // One staged block (or one long unit) of a staged kernel: gather, then rows in the
 // reference order.  `smem_stage` is the block's stage buffer, `xb` the gather buffer.
-template <Kind K, Arith A, int L, bool YMAP>
+template <Kind K, Arith A, int L, bool YMAP, bool OWNX = false>
 __device__ __forceinline__ void staged_block(const StagedArgs & a, const StagedBlock & d, uint8_t * smem_stage, double * xb)
 {
-	if (d.units >= 0) {
+	if (OWNX && d.units >= 0) {
+		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+		int js0 = 0, je0 = 0;
+		if (K == Kind::CSR && (int) threadIdx.x < d.units) {
+			const int64_t r = (int64_t) d.unit0 + threadIdx.x;
+			js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+			je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+		}
+		own_rows<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(smem_stage),
+				reinterpret_cast<const int32_t *>(smem_stage + (size_t) a.cap_al * 8), js0, je0);
+	} else if (d.units >= 0) {
 		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
 		const int off = (int) (d.elem0 - e0);
 		const int cnt = d.elems;
@@ -332,7 +403,7 @@ __device__ __forceinline__ void staged_block(const StagedArgs & a, const StagedB
 	}
 }
 
-template <Kind K, Arith A, int L, bool YMAP>
+template <Kind K, Arith A, int L, bool YMAP, bool OWNX = false>
 __global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
@@ -376,7 +447,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a
 			return;
 		}
 		const StagedBlock d = sdesc[s];
-		staged_block<K, A, L, YMAP>(a, d, smem + (size_t) s * a.stage_bytes, xb);
+		staged_block<K, A, L, YMAP, OWNX>(a, d, smem + (size_t) s * a.stage_bytes, xb);
 		__syncthreads();
 		if (threadIdx.x == 0 && nb < a.nblocks) {
 			sdesc[s] = dnext;
@@ -1016,26 +1087,36 @@ __global__ void __launch_bounds__(256) sliced_kernel(SlicedArgs a)
 
 using StagedFn = void (*)(StagedArgs);
 
-// The staged kernel instance of a handle's format / lane count.
+template <bool OWNX>
+StagedFn pick_staged_t(const Handle & h);
+
+// The staged kernel instance of a handle's format / lane count (kernel 5: rows gather
+// their own x).
 StagedFn pick_staged(const Handle & h)
+{
+	return h.exec_kernel == 5 ? pick_staged_t<true>(h) : pick_staged_t<false>(h);
+}
+
+template <bool OWNX>
+StagedFn pick_staged_t(const Handle & h)
 {
 	const int fmt = h.desc.format;
 	if (fmt == SPMV_FMT_CSR_NAIVE)
-		return staged_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+		return staged_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false, OWNX>;
 	if (fmt == SPMV_FMT_CSR_VEC) {
 		switch (h.desc.vec_len) {
-		case 1: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
-		case 2: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 2, false>;
-		case 4: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 4, false>;
-		case 8: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 8, false>;
-		case 16: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 16, false>;
+		case 1: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 1, false, OWNX>;
+		case 2: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 2, false, OWNX>;
+		case 4: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 4, false, OWNX>;
+		case 8: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 8, false, OWNX>;
+		case 16: return staged_kernel<Kind::CSR, Arith::LANES_FMA, 16, false, OWNX>;
 		}
 		return nullptr;
 	}
 	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
-		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true, OWNX>;
 	if (fmt == SPMV_FMT_SELL)
-		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+		return staged_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false, OWNX>;
 	return nullptr;
 }
 
@@ -1261,7 +1342,7 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	const int fmt = h.desc.format;
 	if (fmt == SPMV_FMT_DIV_RF)
 		return launch_div(h, d_x, d_y, s);
-	if (h.exec_kernel == 2)
+	if (h.exec_kernel == 2 || h.exec_kernel == 6)
 		return launch_warp(h, d_x, d_y, s);
 	if (h.exec_kernel == 1) {
 		SlicedArgs a{};

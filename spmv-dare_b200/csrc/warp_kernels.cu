@@ -76,7 +76,10 @@ __device__ __forceinline__ void warp_issue(const WarpArgs & a, int64_t c, uint8_
 	bulk_g2s(sc, a.cols + e0, cnt * 4u, bar);
 }
 
-template <Kind K, Arith A, int L, bool YMAP>
+// OWNX (slices only): no gather pass and no x buffer -- each lane loads the x entries of
+// its own slice row inside its FMA loop (8 independent loads in flight), so a warp's
+// shared memory holds only its bulk-copy ring and more warps fit on an SM.
+template <Kind K, Arith A, int L, bool YMAP, bool OWNX = false>
 __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
@@ -121,16 +124,18 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 		double * sv = reinterpret_cast<double *>(wsm + (size_t) s * a.stage_bytes) + off;
 		const int32_t * sc = reinterpret_cast<const int32_t *>(wsm + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8) + off;
 		double * xs = xb + off;
-		// gather x for all entries of the chunk
-		#pragma unroll 8
-		for (int e = lane; e < d.elems; e += 32) {
-			const double xv = ldg(a.x + sc[e]);
-			if (A == Arith::SEQ_SPLIT)
-				sv[e] = __dmul_rn(sv[e], xv);
-			else
-				xs[e] = xv;
+		if (!OWNX) {
+			// gather x for all entries of the chunk
+			#pragma unroll 8
+			for (int e = lane; e < d.elems; e += 32) {
+				const double xv = ldg(a.x + sc[e]);
+				if (A == Arith::SEQ_SPLIT)
+					sv[e] = __dmul_rn(sv[e], xv);
+				else
+					xs[e] = xv;
+			}
+			__syncwarp();
 		}
-		__syncwarp();
 		const bool long_unit = (d.flags & (CONT_PREV | CONT_NEXT)) != 0;
 		if (K == Kind::CSR) {
 			if (!long_unit) {
@@ -223,9 +228,15 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 						const int ks = a.ptr[sl] - d.elem0 + r;
 						const int wd = (a.ptr[sl + 1] - a.ptr[sl]) / V;
 						double sum = 0.0;
-						#pragma unroll 4
-						for (int k = 0; k < wd; k++)
-							sum = __fma_rn(sv[ks + k * V], xs[ks + k * V], sum);
+						if (OWNX) {
+							#pragma unroll 8
+							for (int k = 0; k < wd; k++)
+								sum = __fma_rn(sv[ks + k * V], ldg(a.x + sc[ks + k * V]), sum);
+						} else {
+							#pragma unroll 4
+							for (int k = 0; k < wd; k++)
+								sum = __fma_rn(sv[ks + k * V], xs[ks + k * V], sum);
+						}
 						a.y[YMAP ? a.ymap[row] : row] = sum;
 					}
 				}
@@ -234,8 +245,14 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 				if (!(d.flags & CONT_PREV))
 					acc = 0.0;
 				const int kn = d.elems / V;
-				for (int k = 0; k < kn; k++)
-					acc = __fma_rn(sv[k * V + lane], xs[k * V + lane], acc);
+				if (OWNX) {
+					#pragma unroll 8
+					for (int k = 0; k < kn; k++)
+						acc = __fma_rn(sv[k * V + lane], ldg(a.x + sc[k * V + lane]), acc);
+				} else {
+					for (int k = 0; k < kn; k++)
+						acc = __fma_rn(sv[k * V + lane], xs[k * V + lane], acc);
+				}
 				if (!(d.flags & CONT_NEXT)) {
 					const int64_t row = (int64_t) d.unit0 * V + lane;
 					if (row < a.m)
@@ -270,10 +287,13 @@ WarpFn pick_warp(const Handle & h)
 		}
 		return nullptr;
 	}
+	const bool own = h.exec_kernel == 6;
 	if (fmt == SPMV_FMT_SELL)
-		return warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
+		return own ? warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false, true>
+		           : warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false>;
 	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
-		return warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
+		return own ? warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true, true>
+		           : warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true>;
 	return nullptr;
 }
 
@@ -381,6 +401,15 @@ __global__ void warp_ranges_kernel(const WarpChunk * ch, const int64_t * prefix,
 	begin[w] = (int32_t) lo;
 }
 
+// Bytes of a warp's x gather buffer: none when csr_naive stores its products in place or
+// when the slice rows load their own x (kernel 6).
+int warp_xbuf_bytes(const Handle & h, int cap_al)
+{
+	const bool slices = h.desc.format == SPMV_FMT_SELL || h.desc.format == SPMV_FMT_SELL_SORTED ||
+			h.desc.format == SPMV_FMT_SELL_C_S;
+	return (h.desc.format == SPMV_FMT_CSR_NAIVE || (h.exec_kernel == 6 && slices)) ? 0 : cap_al * 8;
+}
+
 }  // namespace
 
 int warp_geometry(Handle & h)
@@ -389,7 +418,7 @@ int warp_geometry(Handle & h)
 	for (;;) {
 		const int cap_al = h.block_cap + 8;
 		const int stage_bytes = (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
-		const int xbuf = (h.desc.format == SPMV_FMT_CSR_NAIVE) ? 0 : cap_al * 8;
+		const int xbuf = warp_xbuf_bytes(h, cap_al);
 		h.warp_bytes = (int) (ceil_div((int64_t) h.stages * stage_bytes + xbuf + 8 * h.stages, 128) * 128);
 		h.smem_bytes = (size_t) h.warp_bytes * (WARP_CTA_THREADS / 32);
 		if (h.smem_bytes <= 220 * 1024)
@@ -428,7 +457,7 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 	if (V > 1 && h.block_cap < V)
 		h.block_cap = V;
 	h.block_cap = (h.block_cap + 7) & ~7;
-	h.stages = h.desc.stages > 0 ? h.desc.stages : 2;
+	h.stages = h.desc.stages > 0 ? h.desc.stages : (h.exec_kernel == 6 ? 3 : 2);
 	SPMV_TRY(warp_geometry(h));
 	int64_t tiles = ceil_div(U, TILE_UNITS);
 	int64_t nch = 0;
@@ -487,7 +516,7 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.stages = h.stages;
 	a.stage_bytes = (int) (ceil_div((int64_t) a.cap_al * 12, 128) * 128);
 	a.warp_bytes = h.warp_bytes;
-	a.xbuf_bytes = (fmt == SPMV_FMT_CSR_NAIVE) ? 0 : a.cap_al * 8;
+	a.xbuf_bytes = warp_xbuf_bytes(h, a.cap_al);
 	a.err = h.d_err;
 	if (fmt == SPMV_FMT_CSR_NAIVE || fmt == SPMV_FMT_CSR_VEC) {
 		a.ptr = h.d_rp;

@@ -26,7 +26,8 @@ def _cta(threads, block):
 
 # 24 classes: the CSR kernel and its staging geometry (threads, row threads, entries per
 # block, stages) -- the choice that depends most on the matrix with these kernels -- and
-# the other formats with their own parameters (lanes, slice height, C and sigma).
+# the other formats with their own parameters (lanes, slice height, C and sigma), each with
+# the kernel it was timed with in the committed database (data/tune_*.npz).
 CLASSES = [
     _ws(160, 64, 768, 3),          # the csr_naive default
     _ws(160, 64, 256, 4),
@@ -44,12 +45,12 @@ CLASSES = [
     {"format": "sell", "vec_len": 4},
     {"format": "sell", "vec_len": 8},
     {"format": "sell_sorted", "vec_len": 4},
-    {"format": "sell_c_s", "sellcs_c": 8, "sellcs_sigma": 256},
-    {"format": "sell_c_s", "sellcs_c": 16, "sellcs_sigma": 512},
-    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 32},
-    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512},
-    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 4096},
-    {"format": "sell_c_s", "sellcs_c": 64, "sellcs_sigma": 1024},
+    {"format": "sell_c_s", "sellcs_c": 8, "sellcs_sigma": 256, "kernel": 0},
+    {"format": "sell_c_s", "sellcs_c": 16, "sellcs_sigma": 512, "kernel": 0},
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 32, "kernel": 0},
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 0},
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 4096, "kernel": 0},
+    {"format": "sell_c_s", "sellcs_c": 64, "sellcs_sigma": 1024, "kernel": 0},
     {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 4},
     {"format": "div_rf"},
 ]

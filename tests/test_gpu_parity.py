@@ -150,6 +150,40 @@ def test_warp_specialised_kernel_rejects_bad_split(sb):
         _mk(sb, g, "sell_c_s", kernel=4, threads=64, block_rows=32, sellcs_c=64, sellcs_sigma=64)
 
 
+@pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s"])
+@pytest.mark.parametrize("threads,block_nnz,stages", [(256, 64, 2), (128, 0, 0), (512, 4096, 3)])
+def test_own_gather_kernel_matches_reference(sb, orc, fmt, threads, block_nnz, stages):
+    """Kernel 5 (row threads load their own x): same y bits as the reference for every
+    golden case; 64-entry blocks force the long-unit path."""
+    for name in golden_names():
+        g = load_golden(name)
+        mf = _mk(sb, g, fmt, kernel=5, threads=threads, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        if fmt == "sell_c_s":
+            arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], 32, 512)
+            ref = orc.sellcs_spmv(arr, mf.m, 32, g["x"])
+        else:
+            ref = g[f"y_{fmt}"]
+        assert _eq_bits(y, ref).size == 0, (name, fmt, threads, block_nnz, stages)
+
+
+@pytest.mark.parametrize("fmt", ["sell", "sell_sorted", "sell_c_s", "csr_naive"])
+@pytest.mark.parametrize("block_nnz,stages", [(64, 2), (0, 0), (1024, 4)])
+def test_warp_own_gather_kernel_matches_reference(sb, orc, fmt, block_nnz, stages):
+    """Kernel 6 (warp-autonomous, slice rows load their own x; CSR takes kernel 2's path):
+    same y bits as the reference for every golden case; 64-entry chunks split long slices."""
+    for name in golden_names():
+        g = load_golden(name)
+        mf = _mk(sb, g, fmt, kernel=6, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        if fmt == "sell_c_s":
+            arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], 32, 512)
+            ref = orc.sellcs_spmv(arr, mf.m, 32, g["x"])
+        else:
+            ref = g[f"y_{fmt}"]
+        assert _eq_bits(y, ref).size == 0, (name, fmt, block_nnz, stages)
+
+
 def test_pipelined_kernel_rejects_oversized_blocks(sb):
     g = load_golden("hand6")
     with pytest.raises(sb.SpmvError):
