@@ -7,6 +7,13 @@
 // batch_kernel (spmv_kernels.cu) drains the queue: CTAs claim blocks through an atomic
 // counter, so the load balances across matrices of any size.  x and y of all matrices are
 // concatenated (offsets in spmv_batch_info).
+//
+// A batch whose matrices are all csr_naive is one SpMV of their block-diagonal matrix over
+// the concatenated x and y: the batch then builds that merged CSR on the device (row
+// pointers and columns shifted by the matrix offsets, each matrix's columns checked against
+// its own n) and runs it as one csr_naive handle -- one launch of the warp-specialised
+// kernel, whose blocks never straddle two matrices' rows.  Every row is still summed in the
+// csr_naive order, so y is bit-identical to the matrices' own handles.
 #include <string.h>
 
 #include <algorithm>
@@ -38,6 +45,7 @@ struct spmv_batch {
 	int cap = 0, stages = 0, threads = 0, grid = 0;
 	size_t smem = 0;
 	int exact = 1;
+	spmv_handle * merged = nullptr;    // all-csr_naive batches: the block-diagonal matrix
 	// cached CUDA graph of (counter reset + kernel) for one (x, y) pair
 	cudaGraphExec_t graph = nullptr;
 	const double * graph_x = nullptr;
@@ -63,6 +71,8 @@ void release(spmv_batch * b)
 {
 	if (b->graph)
 		cudaGraphExecDestroy(b->graph);
+	if (b->merged)
+		spmv_destroy(b->merged);
 	for (spmv_handle * h : b->mats)
 		spmv_destroy(h);
 	for (void * p : b->allocs)
@@ -72,8 +82,116 @@ void release(spmv_batch * b)
 	delete b;
 }
 
+__global__ void merge_rows_kernel(const int32_t * rp, int64_t m, int64_t row_off, int64_t nnz_off, int32_t * out)
+{
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < m)
+		out[row_off + i] = (int32_t) (rp[i] + nnz_off);
+}
+
+// Shifts one matrix's columns by its x offset, flagging any column outside [0, n).
+__global__ void merge_cols_kernel(int32_t * ci, int64_t nnz, int64_t n, int64_t x_off, int * bad)
+{
+	const int64_t j = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= nnz)
+		return;
+	const int32_t c = ci[j];
+	if (c < 0 || (int64_t) c >= n)
+		atomicOr(bad, 1);
+	ci[j] = (int32_t) (c + x_off);
+}
+
+// The block-diagonal csr_naive handle of an all-csr_naive batch.
+int build_merged(spmv_batch * b, int32_t count, const int32_t * const * row_ptrs, const int32_t * const * col_inds,
+		const double * const * values, const int64_t * ms, const int64_t * ns, const spmv_format_desc & d0)
+{
+	int64_t M = 0, N = 0, NNZ = 0, maxm = 0;
+	for (int32_t i = 0; i < count; i++) {
+		if (ms[i] < 0 || ns[i] < 0 || !row_ptrs[i] || row_ptrs[i][0] != 0) {
+			spmv::set_error(SPMV_ERR_CSR, "batch: matrix %d: row_ptr[0] must be 0", i);
+			return SPMV_ERR_CSR;
+		}
+		b->x_off.push_back(N);
+		b->y_off.push_back(M);
+		M += ms[i];
+		N += ns[i];
+		NNZ += row_ptrs[i][ms[i]];
+		maxm = ms[i] > maxm ? ms[i] : maxm;
+	}
+	if (M >= INT32_MAX || N >= INT32_MAX || NNZ >= (int64_t) INT32_MAX - 16) {
+		spmv::set_error(SPMV_ERR_OVERFLOW, "batch: the merged matrix exceeds 32-bit indices");
+		return SPMV_ERR_OVERFLOW;
+	}
+	cudaStream_t s = b->stream;
+	int32_t *rp = nullptr, *ci = nullptr, *tmp = nullptr;
+	double * v = nullptr;
+	int * bad = nullptr;
+	int st = SPMV_OK;
+	auto fail = [&](cudaError_t e) {
+		if (e != cudaSuccess && st == SPMV_OK) {
+			spmv::set_error(e == cudaErrorMemoryAllocation ? SPMV_ERR_NOMEM : SPMV_ERR_CUDA, "batch merge: %s",
+					cudaGetErrorString(e));
+			st = e == cudaErrorMemoryAllocation ? SPMV_ERR_NOMEM : SPMV_ERR_CUDA;
+		}
+	};
+	fail(cudaMalloc((void **) &rp, (M + 1) * sizeof(int32_t)));
+	fail(cudaMalloc((void **) &ci, (NNZ + 1) * sizeof(int32_t)));
+	fail(cudaMalloc((void **) &v, (NNZ + 1) * sizeof(double)));
+	fail(cudaMalloc((void **) &tmp, (maxm + 1) * sizeof(int32_t)));
+	fail(cudaMalloc((void **) &bad, sizeof(int)));
+	if (st == SPMV_OK)
+		fail(cudaMemsetAsync(bad, 0, sizeof(int), s));
+	int64_t nnz_off = 0;
+	for (int32_t i = 0; i < count && st == SPMV_OK; i++) {
+		const int64_t nnz = row_ptrs[i][ms[i]];
+		if (ms[i] > 0) {
+			fail(cudaMemcpyAsync(tmp, row_ptrs[i], ms[i] * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+			merge_rows_kernel<<<(unsigned) spmv::ceil_div(ms[i], 256), 256, 0, s>>>(tmp, ms[i], b->y_off[i], nnz_off, rp);
+			fail(cudaGetLastError());
+		}
+		if (nnz > 0) {
+			fail(cudaMemcpyAsync(ci + nnz_off, col_inds[i], nnz * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+			fail(cudaMemcpyAsync(v + nnz_off, values[i], nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+			merge_cols_kernel<<<(unsigned) spmv::ceil_div(nnz, 256), 256, 0, s>>>(ci + nnz_off, nnz, ns[i], b->x_off[i], bad);
+			fail(cudaGetLastError());
+		}
+		// a pageable source is copied before the call returns, so tmp may be refilled
+		fail(cudaStreamSynchronize(s));
+		nnz_off += nnz;
+	}
+	if (st == SPMV_OK) {
+		const int32_t last = (int32_t) NNZ;
+		fail(cudaMemcpyAsync(rp + M, &last, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+		int hbad = 0;
+		fail(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+		fail(cudaStreamSynchronize(s));
+		if (st == SPMV_OK && hbad) {
+			spmv::set_error(SPMV_ERR_CSR, "batch: a column index is outside its matrix's [0, n)");
+			st = SPMV_ERR_CSR;
+		}
+	}
+	if (st == SPMV_OK) {
+		spmv_format_desc d;
+		spmv_format_desc_init(&d, SPMV_FMT_CSR_NAIVE);
+		d.exact = d0.exact;
+		b->merged = spmv_create_device(rp, ci, v, M, N, NNZ, &d, b->stream, &st);
+	}
+	for (void * p : {(void *) rp, (void *) ci, (void *) v, (void *) tmp, (void *) bad})
+		if (p)
+			cudaFree(p);
+	if (st != SPMV_OK)
+		return st;
+	b->total_x = N;
+	b->total_y = M;
+	b->total_nnz = NNZ;
+	b->nblocks = spmv::handle_of(b->merged)->num_blocks;
+	return SPMV_OK;
+}
+
 int enqueue(spmv_batch * b, const double * d_x, double * d_y, cudaStream_t s)
 {
+	if (b->merged)
+		return spmv_run_device(b->merged, d_x, d_y, s);
 	SPMV_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s));
 	if (b->nblocks == 0)
 		return SPMV_OK;
@@ -109,6 +227,29 @@ spmv_batch * spmv_batch_create(int32_t count, const int32_t * const * row_ptrs, 
 		return nullptr;
 	}
 	spmv_batch * b = new spmv_batch();
+	bool all_csr = count > 0;
+	for (int32_t i = 0; i < count; i++)
+		all_csr = all_csr && descs[i].format == SPMV_FMT_CSR_NAIVE && descs[i].values == SPMV_VALUES_F64;
+	if (all_csr) {
+		cudaGetDevice(&b->device);
+		if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+			spmv::set_error(SPMV_ERR_CUDA, "batch: stream creation failed");
+			st = SPMV_ERR_CUDA;
+		}
+		if (st == SPMV_OK)
+			st = build_merged(b, count, row_ptrs, col_inds, values, ms, ns, descs[0]);
+		if (st == SPMV_OK)
+			st = balloc(b, &b->d_err, 1);
+		if (st == SPMV_OK && cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess)
+			st = SPMV_ERR_CUDA;
+		if (st != SPMV_OK) {
+			release(b);
+			b = nullptr;
+		}
+		if (status)
+			*status = st;
+		return b;
+	}
 	// one staging geometry for the whole batch (that of the first descriptor)
 	b->cap = (count > 0 && descs[0].block_nnz > 0) ? descs[0].block_nnz : 1024;
 	b->cap = (b->cap + 7) & ~7;
@@ -284,6 +425,8 @@ int spmv_batch_sync(spmv_batch * b)
 		return SPMV_ERR_ARG;
 	}
 	SPMV_CUDA_TRY(cudaDeviceSynchronize());
+	if (b->merged)
+		return spmv_sync(b->merged);
 	int e = 0;
 	SPMV_CUDA_TRY(cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
 	if (e == DEV_ERR_TIMEOUT) {

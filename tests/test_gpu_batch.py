@@ -53,3 +53,40 @@ def test_batch_rejects_unbatchable_format(sb):
     mats = _matrices(sb, 2, 9)
     with pytest.raises(sb.SpmvError):
         sb.Batch(mats, ["csr_naive", "div_rf"])
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_all_csr_batch_runs_as_one_block_diagonal_spmv(sb, graph):
+    """An all-csr_naive batch is one SpMV of the block-diagonal matrix (merged on the
+    device, warp-specialised kernel): y bit-identical to each matrix's own handle, with
+    empty and one-row matrices among them."""
+    import torch
+
+    mats = _matrices(sb, 20, 11)
+    mats.insert(5, (np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0), 0, 3))       # no rows
+    mats.insert(9, (np.array([0, 2], np.int32), np.array([0, 4], np.int32), np.array([1.5, -2.0]), 1, 6))
+    b = sb.Batch(mats, ["csr_naive"] * len(mats))
+    assert b.total_nnz == sum(int(m[0][-1]) for m in mats) and b.num_blocks > 0
+    x = np.random.default_rng(5).uniform(-1, 1, b.total_x)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.full((b.total_y,), 5.0, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        b.spmv(xd, yd, graph=graph)
+    b.sync()
+    y = yd.cpu().numpy()
+    for i, (rp, ci, v, m, n) in enumerate(mats):
+        if m == 0:
+            continue
+        mf = sb.csr_to_format(rp, ci, v, m, n, int(rp[-1]), format="csr_naive")
+        xo, yo = b.x_offsets[i], b.y_offsets[i]
+        assert np.array_equal(y[yo:yo + m].view(np.uint64), mf.spmv(x[xo:xo + n]).view(np.uint64)), i
+
+
+def test_all_csr_batch_rejects_column_outside_its_matrix(sb):
+    mats = _matrices(sb, 3, 13)
+    rp, ci, v, m, n = mats[1]
+    ci = ci.copy()
+    ci[0] = n                  # valid in the merged matrix's width, invalid for matrix 1
+    mats[1] = (rp, ci, v, m, n)
+    with pytest.raises(sb.SpmvError):
+        sb.Batch(mats, ["csr_naive"] * 3)
