@@ -108,6 +108,13 @@ class ClockSampler:
                                       stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # nvidia-smi's start-up (seconds on a freshly booted node) can hold the driver and
+        # stall this process's launches: time only once its first sample is written
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 15.0:
+            if os.path.getsize(self.path) > 0 or self.p.poll() is not None:
+                break
+            time.sleep(0.05)
         time.sleep(0.3)
 
     def stop(self):

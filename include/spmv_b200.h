@@ -78,8 +78,8 @@ extern "C" {
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
  *                    threads per CTA), 0 = default.
- *   kernel          -1: the format's default (4 for csr_naive, 6 for SELL-C-sigma with
- *                       C <= 32, 0 otherwise);
+ *   kernel          -1: the format's default (4 for csr_naive, 8 for SELL-C-sigma, 0
+ *                       otherwise);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
  *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);
@@ -91,7 +91,14 @@ extern "C" {
  *                    5: CTA staged kernel whose row threads load their own x, no gather
  *                       phase (every format but DIV-RF);
  *                    6: warp-autonomous kernel whose slice rows load their own x, no x
- *                       buffer (sell, sell_sorted, SELL-C-sigma with C <= 32).  default -1
+ *                       buffer (sell, sell_sorted, SELL-C-sigma with C <= 32);
+ *                    7: FP32 variant only: segmented kernel, 256-entry chunks with Dot2
+ *                       per lane and compensated merges across lanes and chunks (spreads
+ *                       a single very long row over the whole GPU);
+ *                    8: FP64 slices of >= 8 rows: kernel 4 over a copy of
+ *                       the column indices laid out row-major in tiles of 8 slice
+ *                       columns, so a gather warp reads 4 rows x 8 columns (the exported
+ *                       arrays keep the reference layout).                   default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;

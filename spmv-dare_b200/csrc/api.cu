@@ -86,9 +86,17 @@ static int check_desc(const spmv_format_desc & d)
 		return SPMV_ERR_ARG;
 	}
 	if (d.block_nnz < 0 || d.block_nnz > 16384 || d.stages < 0 || d.stages > 8 || d.block_rows < 0 ||
-			d.block_rows > 4096 || d.ctas_per_sm < 0 || d.ctas_per_sm > 32 || d.kernel < -1 || d.kernel > 6 ||
+			d.block_rows > 4096 || d.ctas_per_sm < 0 || d.ctas_per_sm > 32 || d.kernel < -1 || d.kernel > 8 ||
 			!(d.threads == 0 || (d.threads % 32 == 0 && d.threads >= 64 && d.threads <= 512))) {
 		set_error(SPMV_ERR_ARG, "tuning knob out of range");
+		return SPMV_ERR_ARG;
+	}
+	if (d.kernel == 7 && d.values != SPMV_VALUES_F32) {
+		set_error(SPMV_ERR_ARG, "kernel 7 (segmented) is the FP32 variant's kernel");
+		return SPMV_ERR_ARG;
+	}
+	if (d.kernel == 8 && d.values != SPMV_VALUES_F64) {
+		set_error(SPMV_ERR_ARG, "kernel 8 (tiled slices) runs FP64 values");
 		return SPMV_ERR_ARG;
 	}
 	return SPMV_OK;
@@ -202,12 +210,13 @@ static int create_common(Handle & h, const int32_t * rp, const int32_t * ci, con
 	h.nnz = nnz;
 	SPMV_TRY(init_device(h));
 	cudaStream_t s = h.stream;
-	// device copies padded by 8 entries (16-byte bulk-copy granularity of the staged kernel)
+	// device copies padded by SPMV_ENTRY_PAD zero entries (column 0, value 0): the staged
+	// kernels copy whole 16-byte units, the FP32 segmented kernel whole 256-entry chunks
 	SPMV_TRY(h.alloc(&h.d_rp, m + 1));
-	SPMV_TRY(h.alloc(&h.d_ci, nnz + 8));
-	SPMV_TRY(h.alloc(&h.d_v, nnz + 8));
-	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_ci + nnz, 0, 8 * sizeof(int32_t), s));
-	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_v + nnz, 0, 8 * sizeof(double), s));
+	SPMV_TRY(h.alloc(&h.d_ci, nnz + SPMV_ENTRY_PAD));
+	SPMV_TRY(h.alloc(&h.d_v, nnz + SPMV_ENTRY_PAD));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_ci + nnz, 0, SPMV_ENTRY_PAD * sizeof(int32_t), s));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_v + nnz, 0, SPMV_ENTRY_PAD * sizeof(double), s));
 	if (host) {
 		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_rp, rp, (m + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 		if (nnz > 0) {

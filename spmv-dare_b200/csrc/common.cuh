@@ -83,6 +83,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, uint32_t parity)
 	return ok != 0;
 }
 
+// try_wait that suspends the warp in hardware (up to `hint_ns` nanoseconds, or until the
+// phase completes) instead of returning at once: a waiting warp takes no issue slots from
+// the warps that work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t * bar, uint32_t parity, uint32_t hint_ns)
+{
+	uint32_t ok;
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+	    "selp.u32 %0, 1, 0, p;\n\t}"
+	    : "=r"(ok)
+	    : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+	    : "memory");
+	return ok != 0;
+}
+
 // Bounded wait on an mbarrier phase: gives up after ~`budget` clock cycles and returns
 // false (the caller records DEV_ERR_TIMEOUT and leaves), so no wait can spin forever.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t * bar, uint32_t parity, long long budget)
@@ -90,7 +106,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t * bar, uint32_t parit
 	if (mbar_try_wait(bar, parity))
 		return true;
 	long long t0 = clock64();
-	while (!mbar_try_wait(bar, parity)) {
+	while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
 		if (clock64() - t0 > budget)
 			return false;
 	}
@@ -149,7 +165,10 @@ __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b)
 }
 
 // x loads a gather thread of the warp-specialised kernels keeps in flight per round.
-static constexpr int WS_GATHER_SLOTS = 4;
+#ifndef SPMV_WS_GATHER_SLOTS
+#define SPMV_WS_GATHER_SLOTS 4
+#endif
+static constexpr int WS_GATHER_SLOTS = SPMV_WS_GATHER_SLOTS;
 
 static constexpr long long kWaitBudgetCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 

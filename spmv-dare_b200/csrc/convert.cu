@@ -420,6 +420,27 @@ int validate_csr(Handle & h)
 	return SPMV_OK;
 }
 
+// Column indices of the slices in row-major tiles of 8 slice columns (kernel 8).  Entry
+// (row r, column k) of slice s, width W = (P[s + 1] - P[s]) / V, moves from
+// P[s] + k * V + r to P[s] + k8 * V + r * tw + (k - k8), k8 = k & ~7, tw = min(8, W - k8):
+// a permutation inside every slice, so blocks of whole slices and chunks of whole tiles
+// are contiguous ranges of the tiled array too.  One thread per slice row.
+__global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, const int32_t * cols, int32_t * out)
+{
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= ns * V)
+		return;
+	const int64_t sl = i / V;
+	const int r = (int) (i % V);
+	const int64_t b = P[sl];
+	const int W = (int) (((int64_t) P[sl + 1] - b) / V);
+	for (int k = 0; k < W; k++) {
+		const int k8 = k & ~7;
+		const int tw = W - k8 < 8 ? W - k8 : 8;
+		out[b + (int64_t) k8 * V + (int64_t) r * tw + (k - k8)] = cols[b + (int64_t) k * V + r];
+	}
+}
+
 // Kernel choice: -1 = the format's default (the warp-specialised kernel for csr_naive, the
 // warp-autonomous own-gather kernel for SELL-C-sigma with C <= 32, the CTA staged kernel
 // otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
@@ -427,15 +448,17 @@ int validate_csr(Handle & h)
 // warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
 // block's gather overlapping this block's rows; 4 = warp-specialised staged kernel; 5 = CTA
 // staged kernel whose row threads load their own x (no separate gather phase); 6 =
-// warp-autonomous kernel whose slice rows load their own x (slices of <= 32 rows).
+// warp-autonomous kernel whose slice rows load their own x (slices of <= 32 rows); 8 =
+// warp-specialised kernel over the column indices in row-major 8-column tiles (slices of
+// >= 8 rows).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
 	if (k < 0) {
 		if (h.desc.format == SPMV_FMT_CSR_NAIVE)
 			k = 4;
-		else if (h.desc.format == SPMV_FMT_SELL_C_S && V <= 32)
-			k = 6;
+		else if (h.desc.format == SPMV_FMT_SELL_C_S)
+			k = 8;
 		else
 			k = 0;
 	}
@@ -445,19 +468,42 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		k = 0;
 	if (k == 6 && V == 1)
 		k = 2;                      // CSR: the warp kernel's own path
+	if (k == 8 && V < 8)
+		k = 4;                      // narrower slices already give a warp 8 neighbouring columns
 	h.exec_kernel = k;
 	if (k == 1)
 		return SPMV_OK;
 	if (k == 2 || k == 6)
 		return build_warp_chunks(h, d_P, U, V);
 	staged_defaults(h);
-	if ((k == 3 || k == 4) && h.desc.stages == 0)
+	if (k == 3 && h.desc.stages == 0)
 		h.stages = 3;
 	if (k == 4) {
-		// row warps: block_rows threads (default 64); at least one gather warp besides them
+		// defaults measured on the 4M-row matrix: 768-entry blocks, 2 stages, 3 gather warps
+		// and 2 row warps (0.196 ms for csr_naive; 3 stages 0.202 ms)
+		if (h.desc.block_nnz == 0)
+			h.block_cap = 768;
+		if (h.desc.stages == 0)
+			h.stages = 2;
 		if (h.desc.threads == 0)
-			h.threads = 160;              // 3 gather warps + 2 row warps
+			h.threads = 160;
 		h.row_threads = h.desc.block_rows > 0 ? h.desc.block_rows : 64;
+	}
+	if (k == 8) {
+		// defaults measured on the 4M-row matrix with C = 32: one row warp per slice, 2 gather
+		// warps, 512-entry blocks, 2 stages (0.255-0.264 ms; 640-entry blocks 0.28-0.31 ms,
+		// 3 stages 0.38 ms: the CTAs an SM holds set the pace)
+		const int rows = V > 32 ? ((V + 31) / 32) * 32 : 32;
+		if (h.desc.block_nnz == 0)
+			h.block_cap = (8 * V > 512 ? 8 * V : 512);
+		if (h.desc.stages == 0)
+			h.stages = 2;
+		h.row_threads = h.desc.block_rows > 0 ? h.desc.block_rows : rows;
+		if (h.desc.threads == 0)
+			h.threads = h.row_threads + 64;
+	}
+	if (k == 4 || k == 8) {
+		// row warps: block_rows threads; at least one gather warp besides them
 		if (h.row_threads % 32 != 0 || h.row_threads + 32 > h.threads || h.row_threads < V) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: block_rows %d must be a multiple of 32, at least the "
 					"slice height %d and leave a gather warp of %d threads", h.row_threads, V, h.threads);
@@ -466,6 +512,21 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		if (h.block_cap < V) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: block_nnz %d below the slice height %d", h.block_cap, V);
 			return SPMV_ERR_ARG;
+		}
+		if (k == 8) {
+			// chunks of whole 8-column tiles, and the tiled copy of the column indices
+			if (h.block_cap < 8 * V) {
+				set_error(SPMV_ERR_ARG, "tiled kernel: block_nnz %d below one tile of 8 x %d entries", h.block_cap, V);
+				return SPMV_ERR_ARG;
+			}
+			const int32_t * cols = h.desc.format == SPMV_FMT_SELL_C_S ? h.d_scols : h.d_ja;
+			SPMV_TRY(h.alloc(&h.d_tcols, h.stored_elems + 8));
+			SPMV_CUDA_TRY(cudaMemsetAsync(h.d_tcols, 0, (h.stored_elems + 8) * sizeof(int32_t), h.stream));
+			if (U > 0) {
+				tile_cols_kernel<<<(unsigned) ceil_div(U * V, 256), 256, 0, h.stream>>>(d_P, U, V, cols, h.d_tcols);
+				SPMV_CUDA_TRY(cudaGetLastError());
+			}
+			return build_blocks(h, d_P, U, h.row_threads / V, (h.block_cap / (8 * V)) * 8 * V);
 		}
 		// units longer than a block: chunks of whole slice columns, summed in order by one CTA
 		return build_blocks(h, d_P, U, h.row_threads / V, (h.block_cap / V) * V);

@@ -12,6 +12,9 @@ namespace spmv {
 // [elem0, elem0 + elems) are copied to shared memory in one bulk transfer.  units < 0
 // marks a long unit (one row / one slice larger than the staging capacity), processed
 // straight from global memory.
+// Zero entries after the last nonzero of every device copy of the CSR arrays.
+constexpr int64_t SPMV_ENTRY_PAD = 256;
+
 struct StagedBlock {
 	int32_t unit0;
 	int32_t units;
@@ -77,6 +80,14 @@ struct Handle {
 	int32_t * d_ci = nullptr;
 	double * d_v = nullptr;
 	float * d_vf = nullptr;      // FP32 variant values
+	// FP32 segmented kernel (kernel 7): first row of every 256-entry chunk, the rows that
+	// cross a chunk boundary, the empty rows, per-chunk partial sums (head, tail)
+	int32_t * d_chunk_row = nullptr;
+	int32_t * d_cross_rows = nullptr;
+	int32_t * d_empty_rows = nullptr;
+	float2 * d_chunk_head = nullptr;
+	float2 * d_chunk_tail = nullptr;
+	int64_t num_seg_chunks = 0, num_cross_rows = 0, num_empty_rows = 0;
 
 	// staged kernel
 	StagedBlock * d_blocks = nullptr;
@@ -88,8 +99,11 @@ struct Handle {
 	int threads = 256;           // threads per CTA of the staged kernel
 	size_t smem_bytes = 0;
 	int exec_kernel = 0;         // 0 CTA staged, 1 direct sliced, 2 warp-autonomous, 3 pipelined,
-	                             // 4 warp-specialised (gather warps + row warps)
-	int row_threads = 0;         // kernel 4: threads of the row warps (the rest gather)
+	                             // 4 warp-specialised (gather warps + row warps), 5 CTA staged
+	                             // own-gather, 6 warp-autonomous own-gather, 7 FP32 segmented,
+	                             // 8 warp-specialised over tiled slice columns
+	int row_threads = 0;         // kernels 4 and 8: threads of the row warps (the rest gather)
+	int32_t * d_tcols = nullptr; // kernel 8: slice column indices, row-major in 8-column tiles
 
 	// warp-autonomous kernel
 	WarpChunk * d_chunks = nullptr;

@@ -18,6 +18,8 @@
 //                   row, a warp reads 32 consecutive column-major entries per step
 //                   (coalesced), fused multiply-add over the slice width as vfmacc does
 //                   (sellcs_mv_d, sell-C-s/sellcs_mv_kernels_epi.c:209-317).
+#include <algorithm>
+
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -46,6 +48,24 @@ struct StagedArgs {
 	const int64_t * ranges;  // warp-specialised kernel: each CTA's contiguous block range
 	int * err;
 };
+
+// Sequential sum of s[0..n) in index order.
+__device__ __forceinline__ double seq_add(const double * s, int n, double sum)
+{
+	#pragma unroll 4
+	for (int j = 0; j < n; j++)
+		sum = __dadd_rn(sum, s[j]);
+	return sum;
+}
+
+// Sequential fused chain sum = fma(v[j * vs], x[j * xs], sum), j = 0..n-1.
+__device__ __forceinline__ double seq_fma(const double * v, int vs, const double * x, int xs, int n, double sum)
+{
+	#pragma unroll 4
+	for (int j = 0; j < n; j++)
+		sum = __fma_rn(v[j * vs], x[j * xs], sum);
+	return sum;
+}
 
 template <int L>
 __device__ __forceinline__ double lanes_reduce(const double * s)
@@ -252,13 +272,9 @@ __device__ __forceinline__ void block_rows(const StagedArgs & a, const StagedBlo
 			const int je = (u == (int) threadIdx.x) ? je0 : (int) ((int64_t) a.ptr[r + 1] - e0);
 			double sum = 0.0;
 			if (A == Arith::SEQ_SPLIT) {
-				#pragma unroll 4
-				for (int j = js; j < je; j++)
-					sum = __dadd_rn(sum, sv[j]);
+				sum = seq_add(sv + js, je - js, sum);
 			} else if (A == Arith::SEQ_FMA) {
-				#pragma unroll 4
-				for (int j = js; j < je; j++)
-					sum = __fma_rn(sv[j], xb[j], sum);
+				sum = seq_fma(sv + js, 1, xb + js, 1, je - js, sum);
 			} else {
 				double ln[L];
 				#pragma unroll
@@ -288,9 +304,7 @@ __device__ __forceinline__ void block_rows(const StagedArgs & a, const StagedBlo
 			const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
 			const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
 			double acc = 0.0;
-			#pragma unroll 4
-			for (int k = 0; k < w; k++)
-				acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
+			acc = seq_fma(sv + ks, V, xb + ks, V, w, acc);
 			a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
 		}
 	}
@@ -598,23 +612,71 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) pipe_kernel(StagedArgs a)
 }
 
 // Row bounds of row thread `t`'s row in block d, relative to the stage start (CSR).
-template <Kind K>
-__device__ __forceinline__ void first_row_bounds_t(const StagedArgs & a, const StagedBlock & d, int t, int & js0, int & je0)
+// What row thread t needs of block d before the block's gather is done, loaded while it
+// waits: CSR, its row's bounds (relative to the stage start); slices, its slice's start and
+// width; the y index of its row (ymap applied; -1: no row).  Chunk blocks of a slice: the
+// y index of the last chunk's row.
+template <Kind K, bool YMAP>
+__device__ __forceinline__ void row_pre_t(const StagedArgs & a, const StagedBlock & d, int t, int & js0, int & je0,
+		int64_t & yi)
 {
 	js0 = 0;
 	je0 = 0;
-	if (K == Kind::CSR && d.units >= 0 && t < d.units) {
-		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
-		const int64_t r = (int64_t) d.unit0 + t;
-		js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
-		je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+	yi = -1;
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	if (K == Kind::CSR) {
+		if (d.units >= 0 && t < d.units) {
+			const int64_t r = (int64_t) d.unit0 + t;
+			js0 = (int) ((int64_t) __ldg(a.ptr + r) - e0);
+			je0 = (int) ((int64_t) __ldg(a.ptr + r + 1) - e0);
+			yi = r;
+		}
+		return;
 	}
+	const int V = a.V;
+	int64_t row = -1;
+	if (d.units >= 0) {
+		if (t < d.units * V) {
+			const int64_t sl = (int64_t) d.unit0 + t / V;
+			const int64_t p0 = __ldg(a.ptr + sl);
+			js0 = (int) (p0 - e0);
+			je0 = (int) (((int64_t) __ldg(a.ptr + sl + 1) - p0) / V);
+			row = sl * V + t % V;
+		}
+	} else if (((-d.units - 1) & 2) && t < V) {
+		row = (int64_t) d.unit0 * V + t;
+	}
+	if (row >= 0 && row < a.m)
+		yi = (YMAP && a.ymap) ? (int64_t) __ldg(a.ymap + row) : row;
 }
 
-// block_rows for row thread t of nt (the block holds at most nt rows).
-template <Kind K, Arith A, int L, bool YMAP>
+// One slice row over w slice columns staged from entry sb (a slice start, or a chunk start
+// on a tile boundary): values column-major (vp[k * V]), x in the tiled order of the column
+// indices (tile of 8 columns at sb + t8 * V, row `lane` at lane * tw inside it), stored at
+// e + e / 8 so that the 32 rows of a full tile (stride 9 doubles) read without bank
+// conflicts.  One fused multiply-add per column, in column order.
+__device__ __forceinline__ double tiled_row(const double * vp, const double * xb, int sb, int w, int V, int lane,
+		double acc)
+{
+	for (int t8 = 0; t8 < w; t8 += 8) {
+		const int tw = w - t8 < 8 ? w - t8 : 8;
+		const int eb = sb + t8 * V + lane * tw;
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			if (j < tw) {
+				const int e = eb + j;
+				acc = __fma_rn(vp[(t8 + j) * V], xb[e + (e >> 3)], acc);
+			}
+		}
+	}
+	return acc;
+}
+
+// block_rows for row thread t of nt (the block holds at most nt rows).  TX: the x of tiled
+// stage entry e sits at e + e / 8 (ws_kernel); row `lane` of a slice reads tile by tile.
+template <Kind K, Arith A, int L, bool YMAP, bool TX = false>
 __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock & d, const double * sv, const double * xb,
-		int js0, int je0, int t, int nt)
+		int js0, int je0, int64_t yi, int t, int nt)
 {
 	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
 	if (K == Kind::CSR) {
@@ -623,13 +685,9 @@ __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock &
 			const int js = js0, je = je0;
 			double sum = 0.0;
 			if (A == Arith::SEQ_SPLIT) {
-				#pragma unroll 4
-				for (int j = js; j < je; j++)
-					sum = __dadd_rn(sum, sv[j]);
+				sum = seq_add(sv + js, je - js, sum);
 			} else if (A == Arith::SEQ_FMA) {
-				#pragma unroll 4
-				for (int j = js; j < je; j++)
-					sum = __fma_rn(sv[j], xb[j], sum);
+				sum = seq_fma(sv + js, 1, xb + js, 1, je - js, sum);
 			} else {
 				double ln[L];
 				#pragma unroll
@@ -648,21 +706,17 @@ __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock &
 			a.y[r] = sum;
 		}
 	} else {
+		// a block holds at most nt / V slices (row_pre_t loaded this thread's slice and y index)
 		const int V = a.V;
-		const int nrow = d.units * V;
-		for (int u = t; u < nrow; u += nt) {
-			const int64_t sl = (int64_t) d.unit0 + u / V;
-			const int lane = u % V;
-			const int64_t row = sl * V + lane;
-			if (row >= a.m)
-				continue;
-			const int ks = (int) ((int64_t) a.ptr[sl] - e0) + lane;
-			const int w = (a.ptr[sl + 1] - a.ptr[sl]) / V;
+		if (yi >= 0) {
+			const int lane = t % V;
+			const int sb = js0, w = je0, ks = sb + lane;
 			double acc = 0.0;
-			#pragma unroll 4
-			for (int k = 0; k < w; k++)
-				acc = __fma_rn(sv[ks + k * V], xb[ks + k * V], acc);
-			a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
+			if (TX)
+				acc = tiled_row(sv + ks, xb, sb, w, V, lane, acc);
+			else
+				acc = seq_fma(sv + ks, V, xb + ks, V, w, acc);
+			a.y[yi] = acc;
 		}
 	}
 }
@@ -699,9 +753,9 @@ __device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock
 // chunk, bit 1: last).  The unit's running state (sum, lanes) lives in the row thread's
 // registers between consecutive chunks, which the same CTA processes in order, so every
 // row is still summed by one thread in the reference order.
-template <Kind K, Arith A, int L, bool YMAP>
+template <Kind K, Arith A, int L, bool YMAP, bool TX = false>
 __device__ __forceinline__ void ws_chunk(const StagedArgs & a, const StagedBlock & d, const double * sv, const double * xg,
-		int rt, double & acc, double (&ln)[L])
+		int64_t yi, int rt, double & acc, double (&ln)[L])
 {
 	const int flags = -d.units - 1;
 	const int off = d.elem0 & 3;
@@ -716,13 +770,9 @@ __device__ __forceinline__ void ws_chunk(const StagedArgs & a, const StagedBlock
 				ln[l] = 0.0;
 		}
 		if (A == Arith::SEQ_SPLIT) {
-			#pragma unroll 4
-			for (int e = 0; e < d.elems; e++)
-				acc = __dadd_rn(acc, sv[off + e]);
+			acc = seq_add(sv + off, d.elems, acc);
 		} else if (A == Arith::SEQ_FMA) {
-			#pragma unroll 4
-			for (int e = 0; e < d.elems; e++)
-				acc = __fma_rn(sv[off + e], xg[off + e], acc);
+			acc = seq_fma(sv + off, 1, xg + off, 1, d.elems, acc);
 		} else {
 			const int64_t js = a.ptr[r], je = a.ptr[r + 1];
 			const int64_t jv = js + ((je - js) & ~(int64_t) (L - 1));
@@ -752,78 +802,21 @@ __device__ __forceinline__ void ws_chunk(const StagedArgs & a, const StagedBlock
 		if (flags & 1)
 			acc = 0.0;
 		const int kn = d.elems / V;
-		#pragma unroll 4
-		for (int k = 0; k < kn; k++)
-			acc = __fma_rn(sv[off + k * V + rt], xg[off + k * V + rt], acc);
-		if (flags & 2) {
-			const int64_t row = (int64_t) d.unit0 * V + rt;
-			if (row < a.m)
-				a.y[(YMAP && a.ymap) ? a.ymap[row] : row] = acc;
-		}
+		if (TX)
+			acc = tiled_row(sv + rt, xg, 0, kn, V, rt, acc);   // chunks start on a tile boundary, off = 0
+		else
+			acc = seq_fma(sv + off + rt, V, xg + off + rt, V, kn, acc);
+		if ((flags & 2) && yi >= 0)
+			a.y[yi] = acc;
 	}
 }
 
-// Block-table order of the warp-specialised kernel.  A group is a block of whole units or
-// the full run of chunk blocks of one long unit.  CTA c of G walks groups c, c + G,
-// c + 2G, ... (so, as in a round-robin walk, the CTAs work on neighbouring groups at any
-// moment), and its groups are stored contiguously: the table is permuted once at set-up
-// and CTA c's range is [ranges[c], ranges[c + 1]).
-__device__ __forceinline__ bool ws_group_start(const StagedBlock & d)
-{
-	return d.units >= 0 || ((-d.units - 1) & 1);
-}
-
-__device__ __forceinline__ int64_t ws_group_rank(int64_t g, int64_t G, int64_t q, int64_t rem)
-{
-	const int64_t c = g % G;
-	return c * q + (c < rem ? c : rem) + g / G;
-}
-
-__global__ void ws_group_flag_kernel(const StagedBlock * blocks, int64_t nb, int64_t * flag)
-{
-	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (b < nb)
-		flag[b] = ws_group_start(blocks[b]) ? 1 : 0;
-}
-
-__global__ void ws_group_start_kernel(const StagedBlock * blocks, int64_t nb, const int64_t * pos, int64_t * gs)
-{
-	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (b < nb && ws_group_start(blocks[b]))
-		gs[pos[b]] = b;
-	if (b == 0)
-		gs[pos[nb]] = nb;
-}
-
-__global__ void ws_group_size_kernel(const int64_t * gs, int64_t ng, int64_t G, int64_t * size_by_rank)
-{
-	const int64_t g = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (g < ng)
-		size_by_rank[ws_group_rank(g, G, ng / G, ng % G)] = gs[g + 1] - gs[g];
-}
-
-__global__ void ws_permute_kernel(const StagedBlock * in, int64_t nb, const int64_t * pos, const int64_t * gs,
-		const int64_t * off_by_rank, int64_t ng, int64_t G, StagedBlock * out)
-{
-	const int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (b >= nb)
-		return;
-	const StagedBlock d = in[b];
-	const int64_t g = pos[b] + (ws_group_start(d) ? 1 : 0) - 1;
-	out[off_by_rank[ws_group_rank(g, G, ng / G, ng % G)] + (b - gs[g])] = d;
-}
-
-__global__ void ws_ranges_kernel(const int64_t * off_by_rank, int64_t ng, int64_t G, int64_t * ranges)
-{
-	const int64_t c = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (c > G)
-		return;
-	const int64_t q = ng / G, rem = ng % G;
-	int64_t r = c * q + (c < rem ? c : rem);
-	ranges[c] = off_by_rank[r < ng ? r : ng];
-}
-
-template <Kind K, Arith A, int L, bool YMAP>
+// TX (kernel 8, slices only): the column indices are stored row-major in tiles of 8 slice
+// columns (tile_cols_kernel), so 32 consecutive gather threads read 4 rows x 8 neighbouring
+// columns instead of 32 rows x 1 column.  The gather keeps that order (x of stage entry e
+// at e + e / 8) and the row threads walk the tiles (tiled_row).  Blocks start at slice
+// boundaries and chunks at tile boundaries, so off == 0.
+template <Kind K, Arith A, int L, bool YMAP, bool TX = false>
 __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
@@ -836,7 +829,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < S; s++) {
 			mbar_init(&full[s], 1);
-			mbar_init(&prod[s], (uint32_t) ng);
+			mbar_init(&prod[s], (uint32_t) (ng / 32));      // one arrival per gather warp
 		}
 		mbar_fence_init();
 	}
@@ -848,8 +841,10 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		// ---- gather warps
 		const int gt = threadIdx.x;
 		for (int64_t b = b_begin; b < b_end; b++) {
-			if (!mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles)) {
-				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			const bool ok = mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles);
+			if (!__all_sync(0xffffffffu, ok)) {            // the warp leaves together
+				if ((gt & 31) == 0)
+					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 				return;
 			}
 			const StagedBlock d = sdesc[s];
@@ -875,13 +870,17 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 						if (e < d.elems) {
 							if (A == Arith::SEQ_SPLIT)
 								sv[off + e] = __dmul_rn(sv[off + e], xv[k]);   // the reference's rounded product
+							else if (TX)
+								xg[e + (e >> 3)] = xv[k];
 							else
 								xg[off + e] = xv[k];
 						}
 					}
 				}
 			}
-			mbar_arrive(&prod[s]);
+			__syncwarp();                                  // the warp's stores before its arrival
+			if ((gt & 31) == 0)
+				mbar_arrive(&prod[s]);
 			if (++s == S) {
 				s = 0;
 				parity ^= 1u;
@@ -913,7 +912,8 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 			dnext = a.blocks[nb];
 		const StagedBlock d = sdesc[s];
 		int js0 = 0, je0 = 0;
-		first_row_bounds_t<K>(a, d, rt, js0, je0);
+		int64_t yi = -1;
+		row_pre_t<K, YMAP>(a, d, rt, js0, je0, yi);
 		const bool ok = mbar_wait_bounded(&prod[s], parity, kWaitBudgetCycles);
 		if (named_bar_or(1, nr, !ok)) {      // all row threads leave together
 			if (rt == 0)
@@ -922,11 +922,11 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		}
 		uint8_t * st = smem + (size_t) s * a.stage_bytes;
 		if (d.units >= 0)
-			rows_t<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(st),
-					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), js0, je0, rt, nr);
+			rows_t<K, A, L, YMAP, TX>(a, d, reinterpret_cast<const double *>(st),
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), js0, je0, yi, rt, nr);
 		else
-			ws_chunk<K, A, L, YMAP>(a, d, reinterpret_cast<const double *>(st),
-					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), rt, acc, ln);
+			ws_chunk<K, A, L, YMAP, TX>(a, d, reinterpret_cast<const double *>(st),
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), yi, rt, acc, ln);
 		named_bar_sync(1, nr);
 		if (rt == 0 && nb < b_end) {
 			sdesc[s] = dnext;
@@ -1166,12 +1166,31 @@ StagedFn pick_ws(const Handle & h)
 	return nullptr;
 }
 
+// The tiled warp-specialised kernel instance (kernel 8) of a sliced format.
+StagedFn pick_ws_tiled(const Handle & h)
+{
+	const int fmt = h.desc.format;
+	if (fmt == SPMV_FMT_SELL_SORTED || fmt == SPMV_FMT_SELL_C_S)
+		return ws_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, true, true>;
+	if (fmt == SPMV_FMT_SELL)
+		return ws_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false, true>;
+	return nullptr;
+}
+
 // Bytes of one stage of the pipelined kernel (values, columns, and gathered x unless the
 // products are formed in place).
 int pipe_stage_bytes(int format, int cap_al)
 {
 	const int per = (format == SPMV_FMT_CSR_NAIVE) ? 12 : 20;
 	return (int) (ceil_div((int64_t) cap_al * per, 128) * 128);
+}
+
+// Bytes of one stage of the tiled kernel: values, columns and the x buffer (entry e at
+// e + e / 8).
+int tiled_stage_bytes(int cap_al)
+{
+	const int64_t xb = (int64_t) cap_al + ceil_div((int64_t) cap_al, 8);
+	return (int) (ceil_div((int64_t) cap_al * 12 + xb * 8, 128) * 128);
 }
 
 }  // namespace
@@ -1195,50 +1214,111 @@ int batch_occupancy(int threads, size_t smem, int * per_sm)
 	return SPMV_OK;
 }
 
-// Permutes the block table into the warp-specialised kernel's per-CTA group order and
-// writes each CTA's range (h.grid CTAs).
+// Block-table order of the warp-specialised kernels.  A group is a block of whole units or
+// the full run of chunk blocks of one long unit (a CTA keeps the unit's running sums in
+// registers, so a group never splits).  CTA c walks the contiguous range [ranges[c],
+// ranges[c + 1]) of the permuted table.  Groups are given to CTAs by their cost (entries
+// plus a per-block overhead): groups above a quarter of the per-CTA share first, largest
+// first, each to the least-loaded CTA (one 65,280-entry SELL-C-sigma slice is half a CTA's
+// share on the 4M-row matrix); then the rest in matrix order, dealt round-robin over the
+// CTAs still below the share, so CTAs running at the same time work on neighbouring rows.
+// A CTA runs its large groups first.  The table is small (16 bytes a block) and is ordered
+// once on the host at set-up.
 int ws_order_blocks(Handle & h)
 {
 	cudaStream_t s = h.stream;
 	const int64_t nb = h.num_blocks, G = h.grid;
 	SPMV_TRY(h.alloc(&h.d_cta_ranges, G + 1));
-	DevBuf flag, pos, gs, sz, off, tmp;
-	SPMV_TRY(flag.alloc((nb + 1) * sizeof(int64_t), s));
-	SPMV_TRY(pos.alloc((nb + 1) * sizeof(int64_t), s));
-	const unsigned gb = (unsigned) ceil_div(nb > 0 ? nb : 1, 256);
-	ws_group_flag_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, flag.as<int64_t>());
-	SPMV_CUDA_TRY(cudaGetLastError());
-	SPMV_TRY(scan_exclusive(flag.as<int64_t>(), pos.as<int64_t>(), nb, s));
-	int64_t ng = 0;
-	SPMV_CUDA_TRY(cudaMemcpyAsync(&ng, pos.as<int64_t>() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
-	SPMV_TRY(gs.alloc((ng + 1) * sizeof(int64_t), s));
-	SPMV_TRY(sz.alloc((ng + 1) * sizeof(int64_t), s));
-	SPMV_TRY(off.alloc((ng + 1) * sizeof(int64_t), s));
-	SPMV_TRY(tmp.alloc((nb + 1) * sizeof(StagedBlock), s));
-	ws_group_start_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, pos.as<int64_t>(), gs.as<int64_t>());
-	SPMV_CUDA_TRY(cudaGetLastError());
-	if (ng > 0) {
-		ws_group_size_kernel<<<(unsigned) ceil_div(ng, 256), 256, 0, s>>>(gs.as<int64_t>(), ng, G, sz.as<int64_t>());
-		SPMV_CUDA_TRY(cudaGetLastError());
-	}
-	SPMV_TRY(scan_exclusive(sz.as<int64_t>(), off.as<int64_t>(), ng, s));
-	ws_permute_kernel<<<gb, 256, 0, s>>>(h.d_blocks, nb, pos.as<int64_t>(), gs.as<int64_t>(), off.as<int64_t>(), ng, G,
-			tmp.as<StagedBlock>());
-	SPMV_CUDA_TRY(cudaGetLastError());
+	std::vector<StagedBlock> hb((size_t) nb);
 	if (nb > 0)
-		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_blocks, tmp.p, nb * sizeof(StagedBlock), cudaMemcpyDeviceToDevice, s));
-	ws_ranges_kernel<<<(unsigned) ceil_div(G + 1, 256), 256, 0, s>>>(off.as<int64_t>(), ng, G, h.d_cta_ranges);
-	SPMV_CUDA_TRY(cudaGetLastError());
+		SPMV_CUDA_TRY(cudaMemcpyAsync(hb.data(), h.d_blocks, nb * sizeof(StagedBlock), cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	constexpr int64_t BLOCK_OVERHEAD = 64;       // entries' worth of hand-off cost per block
+	std::vector<int64_t> gs;                     // group starts, then nb
+	std::vector<int64_t> cost;
+	for (int64_t b = 0; b < nb; b++) {
+		const StagedBlock & d = hb[(size_t) b];
+		if (d.units >= 0 || ((-d.units - 1) & 1)) {
+			gs.push_back(b);
+			cost.push_back(0);
+		}
+		cost.back() += d.elems + BLOCK_OVERHEAD;
+	}
+	const int64_t ng = (int64_t) cost.size();
+	gs.push_back(nb);
+	int64_t total = 0;
+	for (int64_t c : cost)
+		total += c;
+	const double share = (double) total / (double) G;
+	std::vector<int64_t> load((size_t) G, 0);
+	std::vector<int32_t> owner((size_t) ng, -1);
+	std::vector<int64_t> big;
+	for (int64_t g = 0; g < ng; g++)
+		if ((double) cost[(size_t) g] > 0.25 * share)
+			big.push_back(g);
+	std::stable_sort(big.begin(), big.end(), [&](int64_t a, int64_t b) { return cost[(size_t) a] > cost[(size_t) b]; });
+	auto least = [&]() {
+		int64_t c = 0;
+		for (int64_t k = 1; k < G; k++)
+			if (load[(size_t) k] < load[(size_t) c])
+				c = k;
+		return c;
+	};
+	for (int64_t g : big) {
+		const int64_t c = least();
+		owner[(size_t) g] = (int32_t) c;
+		load[(size_t) c] += cost[(size_t) g];
+	}
+	int64_t c = 0;
+	for (int64_t g = 0; g < ng; g++) {
+		if (owner[(size_t) g] >= 0)
+			continue;
+		int64_t tries = 0;
+		while ((double) load[(size_t) c] >= share && tries < G) {
+			c = (c + 1) % G;
+			tries++;
+		}
+		if (tries == G)
+			c = least();
+		owner[(size_t) g] = (int32_t) c;
+		load[(size_t) c] += cost[(size_t) g];
+		c = (c + 1) % G;
+	}
+	// each CTA's blocks: its large groups (largest first), then its other groups in order
+	std::vector<int64_t> ranges((size_t) G + 1, 0);
+	for (int64_t g = 0; g < ng; g++)
+		ranges[(size_t) owner[(size_t) g] + 1] += gs[(size_t) g + 1] - gs[(size_t) g];
+	for (int64_t k = 0; k < G; k++)
+		ranges[(size_t) k + 1] += ranges[(size_t) k];
+	std::vector<int64_t> fill(ranges.begin(), ranges.end() - 1);
+	std::vector<StagedBlock> out((size_t) nb);
+	auto place = [&](int64_t g) {
+		int64_t & f = fill[(size_t) owner[(size_t) g]];
+		for (int64_t b = gs[(size_t) g]; b < gs[(size_t) g + 1]; b++)
+			out[(size_t) f++] = hb[(size_t) b];
+	};
+	std::vector<char> is_big((size_t) ng, 0);
+	for (int64_t g : big) {
+		is_big[(size_t) g] = 1;
+		place(g);
+	}
+	for (int64_t g = 0; g < ng; g++)
+		if (!is_big[(size_t) g])
+			place(g);
+	if (nb > 0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_blocks, out.data(), nb * sizeof(StagedBlock), cudaMemcpyHostToDevice, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_cta_ranges, ranges.data(), (G + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
 	return SPMV_OK;
 }
 
 // Grid / shared-memory geometry of the staged kernel for this handle.
 int staged_geometry(Handle & h)
 {
-	if (h.exec_kernel == 4) {
+	if (h.exec_kernel == 4 || h.exec_kernel == 8) {
 		const int cap_al = h.block_cap + 8;
-		const int stage_bytes = pipe_stage_bytes(h.desc.format, cap_al);
+		const int stage_bytes = h.exec_kernel == 8 ? tiled_stage_bytes(cap_al)
+		                                           : pipe_stage_bytes(h.desc.format, cap_al);
 		const int max_stages = (220 * 1024 - 128) / stage_bytes;
 		if (max_stages < 2) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: staging block of %d entries exceeds shared memory",
@@ -1251,7 +1331,8 @@ int staged_geometry(Handle & h)
 			h.stages = 2;
 		h.smem_bytes = (size_t) h.stages * stage_bytes + (size_t) h.stages * 16;
 		// FP32-value handles run ws_f32_kernel (fp32.cu), whose stage is also 12 B per entry
-		const void * kern = (h.desc.values == SPMV_VALUES_F32) ? ws_f32_kernel_fn() : (const void *) pick_ws(h);
+		const void * kern = (h.desc.values == SPMV_VALUES_F32) ? ws_f32_kernel_fn()
+		                    : (const void *) (h.exec_kernel == 8 ? pick_ws_tiled(h) : pick_ws(h));
 		if (!kern) {
 			set_error(SPMV_ERR_ARG, "no warp-specialised kernel for format %d with vec_len %d", h.desc.format,
 					h.desc.vec_len);
@@ -1420,6 +1501,12 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	} else if (h.exec_kernel == 4) {
 		kern = pick_ws(h);
 		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
+		a.row_threads = h.row_threads;
+		a.ranges = h.d_cta_ranges;
+	} else if (h.exec_kernel == 8) {
+		kern = pick_ws_tiled(h);
+		a.cols = h.d_tcols;
+		a.stage_bytes = tiled_stage_bytes(a.cap_al);
 		a.row_threads = h.row_threads;
 		a.ranges = h.d_cta_ranges;
 	}

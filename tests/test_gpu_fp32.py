@@ -22,12 +22,14 @@ def _run(sb, rp, ci, v, x, **kw):
     return mf, y32, y64
 
 
-@pytest.mark.parametrize("kernel", [-1, 0])
+@pytest.mark.parametrize("kernel", [-1, 4, 0, 7])
 @pytest.mark.parametrize("name", golden_names())
 def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
-    """Default kernel (warp-specialised): every row, long ones included, is one sequential
-    Dot2 chain, bit-identical to the oracle.  Kernel 0 reduces rows longer than one staged
-    block with a compensated tree: those rows are checked by tolerance only."""
+    """Kernel 4 (warp-specialised, the default): every row, long ones included, is one
+    sequential Dot2 chain, bit-identical to the oracle.  Kernel 0 reduces rows longer than
+    one staged block with a compensated tree: only the other rows are bit-identical.
+    Kernel 7 (segmented: Dot2 per lane, compensated merges across lanes and chunks) fixes
+    another order: it is held to the error bound and to within 2e-7 of the oracle's rows."""
     g = load_golden(name)
     rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
     mf, y32, y64 = _run(sb, rp, ci, v, x, kernel=kernel)
@@ -35,10 +37,44 @@ def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
     assert np.array_equal(mf.export("values"), v.astype(np.float32))
     ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
     lens = np.diff(rp)
-    short = lens <= 2048 if kernel == 0 else np.ones(lens.size, bool)
-    assert np.array_equal(y32[short].view(np.uint32), ref[short].view(np.uint32))
-    assert np.array_equal(y64.astype(np.float32).view(np.uint32), y32.view(np.uint32))
     gold, absy = orc.csr_gold(rp, ci, v, x)
+    if kernel == 7:
+        scale = np.maximum(np.abs(ref.astype(np.float64)), absy)
+        assert np.all(np.abs(y32.astype(np.float64) - ref) <= 2e-7 * np.maximum(scale, 1e-30))
+    else:
+        short = lens <= 2048 if kernel == 0 else np.ones(lens.size, bool)
+        assert np.array_equal(y32[short].view(np.uint32), ref[short].view(np.uint32))
+    assert np.array_equal(y64.astype(np.float32).view(np.uint32), y32.view(np.uint32))
+    assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
+
+
+@pytest.mark.parametrize("kernel", [7, -1])
+@pytest.mark.parametrize("case", ["long_rows", "empty_rows", "chunk_multiple", "one_long_row"])
+def test_fp32_segmented_kernel_edge_cases(sb, orc, case, kernel):
+    """Kernel 7 on rows across many 256-entry chunks, empty rows (leading, inner, trailing),
+    nnz an exact multiple of the chunk, a single row spanning every chunk (and the default
+    kernel on the same cases): within the error bound, empty rows zero."""
+    rng = np.random.default_rng(len(case))
+    if case == "long_rows":
+        lens = rng.integers(0, 3000, 200)
+    elif case == "empty_rows":
+        lens = np.where(rng.random(3000) < 0.4, 0, rng.integers(1, 40, 3000))
+        lens[:7] = 0
+        lens[-11:] = 0
+    elif case == "chunk_multiple":
+        lens = np.full(1024, 64)                        # nnz = 65536 = 256 chunks of 256
+    else:
+        lens = np.array([5000])
+    n = 8192
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens]).astype(np.int32) \
+        if lens.sum() else np.zeros(0, np.int32)
+    v = rng.uniform(-1, 1, int(rp[-1]))
+    x = rng.uniform(-1, 1, n)
+    mf = sb.csr_to_format(rp, ci, v, rp.size - 1, n, int(rp[-1]), format="csr_naive", value_type="f32", kernel=kernel)
+    y32 = mf.spmv(x.astype(np.float32), np.full(mf.m, 7.0, np.float32))
+    gold, absy = orc.csr_gold(rp, ci, v, x)
+    assert np.all(y32[lens == 0] == 0.0)
     assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
 
 
