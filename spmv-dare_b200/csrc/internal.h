@@ -186,6 +186,7 @@ int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
 int convert_f32(Handle & h);
 const void * ws_f32_kernel_fn();   // the FP32 warp-specialised kernel (geometry queries)
+int f32ws_stage_bytes(int cap_al);  // its stage size: 8 bytes per staged entry
 int run_mixed_noalloc(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
 int convert_vector_d2f(const double * in, float * out, int64_t n, cudaStream_t s);
 int convert_vector_f2d(const float * in, double * out, int64_t n, cudaStream_t s);

@@ -1318,7 +1318,8 @@ int staged_geometry(Handle & h)
 	if (h.exec_kernel == 4 || h.exec_kernel == 8) {
 		const int cap_al = h.block_cap + 8;
 		const int stage_bytes = h.exec_kernel == 8 ? tiled_stage_bytes(cap_al)
-		                                           : pipe_stage_bytes(h.desc.format, cap_al);
+		                        : h.desc.values == SPMV_VALUES_F32 ? f32ws_stage_bytes(cap_al)
+		                        : pipe_stage_bytes(h.desc.format, cap_al);
 		const int max_stages = (220 * 1024 - 128) / stage_bytes;
 		if (max_stages < 2) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: staging block of %d entries exceeds shared memory",
