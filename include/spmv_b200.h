@@ -98,7 +98,10 @@ extern "C" {
  *                    8: FP64 slices of >= 8 rows: kernel 4 over a copy of
  *                       the column indices laid out row-major in tiles of 8 slice
  *                       columns, so a gather warp reads 4 rows x 8 columns (the exported
- *                       arrays keep the reference layout).                   default -1
+ *                       arrays keep the reference layout);
+ *                    9: FP64 slices of exactly 32 rows: kernel 6's warp-owned slices over
+ *                       the same tiles; each warp loads x tile by tile and transposes it
+ *                       between lanes (no x buffer).                        default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;

@@ -441,6 +441,19 @@ __global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, const int
 	}
 }
 
+// The tiled copy of a sliced format's column indices (kernels 8 and 9).
+static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
+{
+	const int32_t * cols = h.desc.format == SPMV_FMT_SELL_C_S ? h.d_scols : h.d_ja;
+	SPMV_TRY(h.alloc(&h.d_tcols, h.stored_elems + 8));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_tcols, 0, (h.stored_elems + 8) * sizeof(int32_t), h.stream));
+	if (U > 0) {
+		tile_cols_kernel<<<(unsigned) ceil_div(U * V, 256), 256, 0, h.stream>>>(d_P, U, V, cols, h.d_tcols);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	return SPMV_OK;
+}
+
 // Kernel choice: -1 = the format's default (the warp-specialised kernel for csr_naive, the
 // warp-autonomous own-gather kernel for SELL-C-sigma with C <= 32, the CTA staged kernel
 // otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
@@ -450,7 +463,8 @@ __global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, const int
 // staged kernel whose row threads load their own x (no separate gather phase); 6 =
 // warp-autonomous kernel whose slice rows load their own x (slices of <= 32 rows); 8 =
 // warp-specialised kernel over the column indices in row-major 8-column tiles (slices of
-// >= 8 rows).
+// >= 8 rows); 9 = warp-autonomous kernel over the same tiles, x transposed between lanes
+// (slices of exactly 32 rows).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
@@ -470,11 +484,17 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		k = 2;                      // CSR: the warp kernel's own path
 	if (k == 8 && V < 8)
 		k = 4;                      // narrower slices already give a warp 8 neighbouring columns
+	if (k == 9 && V != 32)
+		k = V >= 8 ? 8 : 4;         // kernel 9's lane transpose takes slices of exactly 32 rows
 	h.exec_kernel = k;
 	if (k == 1)
 		return SPMV_OK;
 	if (k == 2 || k == 6)
 		return build_warp_chunks(h, d_P, U, V);
+	if (k == 9) {
+		SPMV_TRY(build_tiled_cols(h, d_P, U, V));
+		return build_warp_chunks(h, d_P, U, V);
+	}
 	staged_defaults(h);
 	if (k == 3 && h.desc.stages == 0)
 		h.stages = 3;
@@ -519,13 +539,7 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 				set_error(SPMV_ERR_ARG, "tiled kernel: block_nnz %d below one tile of 8 x %d entries", h.block_cap, V);
 				return SPMV_ERR_ARG;
 			}
-			const int32_t * cols = h.desc.format == SPMV_FMT_SELL_C_S ? h.d_scols : h.d_ja;
-			SPMV_TRY(h.alloc(&h.d_tcols, h.stored_elems + 8));
-			SPMV_CUDA_TRY(cudaMemsetAsync(h.d_tcols, 0, (h.stored_elems + 8) * sizeof(int32_t), h.stream));
-			if (U > 0) {
-				tile_cols_kernel<<<(unsigned) ceil_div(U * V, 256), 256, 0, h.stream>>>(d_P, U, V, cols, h.d_tcols);
-				SPMV_CUDA_TRY(cudaGetLastError());
-			}
+			SPMV_TRY(build_tiled_cols(h, d_P, U, V));
 			return build_blocks(h, d_P, U, h.row_threads / V, (h.block_cap / (8 * V)) * 8 * V);
 		}
 		// units longer than a block: chunks of whole slice columns, summed in order by one CTA

@@ -16,6 +16,8 @@
 //     (csr_cross_row_similarity)
 //   9 avg clustering: mean over rows of groups of consecutive columns / degree
 // All sums run in FP64 with atomics (order-independent up to FP64 rounding).
+#include <mutex>
+
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -251,24 +253,39 @@ inline unsigned blocks_for(int64_t n, int t)
 int features_device(const int32_t * d_rp, const int32_t * d_ci, int64_t m, int64_t n, int64_t nnz, double * out,
 		cudaStream_t s)
 {
-	DevBuf sums, mx;
-	SPMV_TRY(sums.alloc(F_NSUMS * sizeof(double), s));
-	SPMV_TRY(mx.alloc(sizeof(unsigned long long), s));
-	SPMV_CUDA_TRY(cudaMemsetAsync(sums.p, 0, F_NSUMS * sizeof(double), s));
-	SPMV_CUDA_TRY(cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), s));
+	// one persistent scratch per device (the sums, then the maximum degree), so a query makes
+	// no allocation: an allocation per call costs more than the whole computation
+	static std::mutex mtx;
+	static void * scratch[64] = {};
+	constexpr size_t SCRATCH = F_NSUMS * sizeof(double) + sizeof(unsigned long long);
+	int dev = 0;
+	SPMV_CUDA_TRY(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= 64) {
+		set_error(SPMV_ERR_ARG, "device index %d out of range", dev);
+		return SPMV_ERR_ARG;
+	}
+	std::lock_guard<std::mutex> lock(mtx);
+	if (!scratch[dev])
+		SPMV_CUDA_TRY(cudaMalloc(&scratch[dev], SCRATCH));
+	double * sums = static_cast<double *>(scratch[dev]);
+	unsigned long long * mx = reinterpret_cast<unsigned long long *>(sums + F_NSUMS);
+	SPMV_CUDA_TRY(cudaMemsetAsync(scratch[dev], 0, SCRATCH, s));
 	if (m > 0) {
 		int64_t grid = blocks_for(m, FEAT_THREADS / 32);     // a warp per row
 		if (grid > 2048)
 			grid = 2048;
-		features_kernel<<<(unsigned) grid, FEAT_THREADS, 0, s>>>(d_rp, d_ci, m, n, sums.as<double>(),
-				mx.as<unsigned long long>());
+		features_kernel<<<(unsigned) grid, FEAT_THREADS, 0, s>>>(d_rp, d_ci, m, n, sums, mx);
 		SPMV_CUDA_TRY(cudaGetLastError());
 	}
-	double h[F_NSUMS];
-	unsigned long long hmx = 0;
-	SPMV_CUDA_TRY(cudaMemcpyAsync(h, sums.p, sizeof(h), cudaMemcpyDeviceToHost, s));
-	SPMV_CUDA_TRY(cudaMemcpyAsync(&hmx, mx.p, sizeof(hmx), cudaMemcpyDeviceToHost, s));
+	struct {
+		double h[F_NSUMS];
+		unsigned long long hmx;
+	} r;
+	static_assert(sizeof(r) == SCRATCH, "scratch layout");
+	SPMV_CUDA_TRY(cudaMemcpyAsync(&r, scratch[dev], SCRATCH, cudaMemcpyDeviceToHost, s));
 	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	const double * h = r.h;
+	const unsigned long long hmx = r.hmx;
 	const double md = m > 0 ? (double) m : 1.0;
 	const double avg = h[F_DEG] / md;
 	const double var = h[F_DEG2] / md - avg * avg;

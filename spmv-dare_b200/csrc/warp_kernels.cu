@@ -270,6 +270,132 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 	}
 }
 
+
+// ------------------------------------------------------------------ tiled warp kernel (kernel 9)
+// 32-row slices whose column indices are stored row-major in tiles of 8 slice columns
+// (tile_cols_kernel).  A warp owns its slices as kernel 6 does, but loads x in the tiled
+// order: load q of lane L is tile entry q * 32 + L, row 4q + L / 8, column L % 8, so a warp
+// request covers 4 rows x 8 neighbouring columns (about 7 distinct sectors on the 4M-row
+// matrix, against 24 for 32 rows x 1 column).  An 8 x 8 transpose between the lanes of
+// each group of 8 and their registers (three shfl.xor stages) then leaves x(row, t8 + j) in
+// register j of lane L, row = 4 (L % 8) + L / 8, which sums its row from the column-major
+// values in the stage: no x buffer in shared memory.  The slice's narrower last tile
+// (width tw < 8, rows at r * tw) is loaded row by row.
+__device__ __forceinline__ void transpose8(double (&X)[8], int lane)
+{
+	#pragma unroll
+	for (int b = 1; b < 8; b <<= 1) {
+		const bool up = (lane & b) != 0;
+		#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			if (q & b)
+				continue;
+			const double send = up ? X[q] : X[q | b];
+			const double recv = __shfl_xor_sync(0xffffffffu, send, b);
+			if (up)
+				X[q] = recv;
+			else
+				X[q | b] = recv;
+		}
+	}
+}
+
+template <bool YMAP>
+__global__ void __launch_bounds__(WARP_CTA_THREADS) tiled_warp_kernel(WarpArgs a)
+{
+	extern __shared__ __align__(128) uint8_t smem[];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const int64_t w = (int64_t) blockIdx.x * (blockDim.x >> 5) + wib;
+	uint8_t * wsm = smem + (size_t) wib * a.warp_bytes;
+	uint64_t * bars = reinterpret_cast<uint64_t *>(wsm + (size_t) a.stages * a.stage_bytes);
+	if (w >= a.nwarps)
+		return;
+	const int64_t cb = a.warp_begin[w], ce = a.warp_begin[w + 1];
+	if (cb >= ce)
+		return;
+	if (lane == 0) {
+		for (int s = 0; s < a.stages; s++)
+			mbar_init(&bars[s], 1);
+		mbar_fence_init();
+	}
+	__syncwarp();
+	if (lane == 0)
+		for (int s = 0; s < a.stages && cb + s < ce; s++)
+			warp_issue(a, cb + s, wsm, &bars[s], s);
+	const int R = 4 * (lane & 7) + (lane >> 3);     // this lane's slice row
+	double acc = 0.0;
+	int s = 0;
+	uint32_t parity = 0;
+	for (int64_t c = cb; c < ce; c++) {
+		const WarpChunk d = a.chunks[c];
+		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
+		if (!__all_sync(0xffffffffu, ok)) {
+			if (lane == 0)
+				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+			return;
+		}
+		// chunks start at slice starts or tile boundaries (multiples of 32 entries): off == 0
+		const double * sv = reinterpret_cast<const double *>(wsm + (size_t) s * a.stage_bytes);
+		const int32_t * sc = reinterpret_cast<const int32_t *>(wsm + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+		if (!(d.flags & CONT_PREV))
+			acc = 0.0;
+		const int wd = d.elems >> 5;
+		const int full = wd & ~7;
+		int t8 = 0;
+		for (; t8 + 16 <= full; t8 += 16) {                 // two tiles' loads in flight
+			double X[8], Y[8];
+			#pragma unroll
+			for (int q = 0; q < 8; q++) {
+				X[q] = ldg(a.x + sc[t8 * 32 + q * 32 + lane]);
+				Y[q] = ldg(a.x + sc[(t8 + 8) * 32 + q * 32 + lane]);
+			}
+			transpose8(X, lane);
+			#pragma unroll
+			for (int j = 0; j < 8; j++)
+				acc = __fma_rn(sv[(t8 + j) * 32 + R], X[j], acc);
+			transpose8(Y, lane);
+			#pragma unroll
+			for (int j = 0; j < 8; j++)
+				acc = __fma_rn(sv[(t8 + 8 + j) * 32 + R], Y[j], acc);
+		}
+		if (t8 < full) {
+			double X[8];
+			#pragma unroll
+			for (int q = 0; q < 8; q++)
+				X[q] = ldg(a.x + sc[t8 * 32 + q * 32 + lane]);
+			transpose8(X, lane);
+			#pragma unroll
+			for (int j = 0; j < 8; j++)
+				acc = __fma_rn(sv[(t8 + j) * 32 + R], X[j], acc);
+			t8 += 8;
+		}
+		if (t8 < wd) {                                      // the slice's narrower last tile
+			const int tw = wd - t8;
+			double X[8];
+			#pragma unroll
+			for (int j = 0; j < 8; j++)
+				X[j] = j < tw ? ldg(a.x + sc[t8 * 32 + R * tw + j]) : 0.0;
+			#pragma unroll
+			for (int j = 0; j < 8; j++)
+				if (j < tw)
+					acc = __fma_rn(sv[(t8 + j) * 32 + R], X[j], acc);
+		}
+		if (!(d.flags & CONT_NEXT)) {
+			const int64_t row = (int64_t) d.unit0 * 32 + R;
+			if (row < a.m)
+				a.y[YMAP ? a.ymap[row] : row] = acc;
+		}
+		__syncwarp();
+		if (lane == 0 && c + a.stages < ce)
+			warp_issue(a, c + a.stages, wsm, &bars[s], s);
+		if (++s == a.stages) {
+			s = 0;
+			parity ^= 1u;
+		}
+	}
+}
+
 using WarpFn = void (*)(WarpArgs);
 
 WarpFn pick_warp(const Handle & h)
@@ -287,6 +413,8 @@ WarpFn pick_warp(const Handle & h)
 		}
 		return nullptr;
 	}
+	if (h.exec_kernel == 9)
+		return fmt == SPMV_FMT_SELL ? tiled_warp_kernel<false> : tiled_warp_kernel<true>;
 	const bool own = h.exec_kernel == 6;
 	if (fmt == SPMV_FMT_SELL)
 		return own ? warp_kernel<Kind::SLICED, Arith::SEQ_FMA, 1, false, true>
@@ -302,10 +430,11 @@ constexpr int TILE_UNITS = 1024;
 
 // Chunks of one tile of units: normal chunks pack whole units (at most 32 rows and `cap`
 // entries); a unit larger than `cap` is cut into consecutive chunks (CSR: runs of entries;
-// slices: runs of whole slice columns) flagged CONT_PREV / CONT_NEXT.
+// slices: runs of whole slice columns, in multiples of `gran` columns) flagged CONT_PREV /
+// CONT_NEXT.
 template <bool WRITE>
-__global__ void warp_chunks_kernel(const int32_t * P, int64_t U, int V, int cap, int64_t * counts, const int64_t * offs,
-		WarpChunk * out)
+__global__ void warp_chunks_kernel(const int32_t * P, int64_t U, int V, int gran, int cap, int64_t * counts,
+		const int64_t * offs, WarpChunk * out)
 {
 	int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	int64_t u = t * TILE_UNITS;
@@ -318,7 +447,7 @@ __global__ void warp_chunks_kernel(const int32_t * P, int64_t U, int V, int cap,
 	while (u < end) {
 		const int64_t len = (int64_t) P[u + 1] - P[u];
 		if (len > cap) {
-			const int64_t step = (V == 1) ? cap : (int64_t) (cap / V) * V;
+			const int64_t step = (V == 1) ? cap : (int64_t) (cap / (V * gran)) * V * gran;
 			for (int64_t c0 = 0; c0 < len; c0 += step) {
 				const int64_t cl = (len - c0) < step ? (len - c0) : step;
 				if (WRITE) {
@@ -407,7 +536,8 @@ int warp_xbuf_bytes(const Handle & h, int cap_al)
 {
 	const bool slices = h.desc.format == SPMV_FMT_SELL || h.desc.format == SPMV_FMT_SELL_SORTED ||
 			h.desc.format == SPMV_FMT_SELL_C_S;
-	return (h.desc.format == SPMV_FMT_CSR_NAIVE || (h.exec_kernel == 6 && slices)) ? 0 : cap_al * 8;
+	return (h.desc.format == SPMV_FMT_CSR_NAIVE || ((h.exec_kernel == 6 || h.exec_kernel == 9) && slices)) ? 0
+	                                                                                           : cap_al * 8;
 }
 
 }  // namespace
@@ -453,11 +583,13 @@ int warp_geometry(Handle & h)
 int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	cudaStream_t s = h.stream;
+	// kernel 9 cuts long slices at 8-column tile boundaries
+	const int gran = h.exec_kernel == 9 ? 8 : 1;
 	h.block_cap = h.desc.block_nnz > 0 ? h.desc.block_nnz : 512;
-	if (V > 1 && h.block_cap < V)
-		h.block_cap = V;
+	if (V > 1 && h.block_cap < V * gran)
+		h.block_cap = V * gran;
 	h.block_cap = (h.block_cap + 7) & ~7;
-	h.stages = h.desc.stages > 0 ? h.desc.stages : (h.exec_kernel == 6 ? 3 : 2);
+	h.stages = h.desc.stages > 0 ? h.desc.stages : (h.exec_kernel == 6 || h.exec_kernel == 9 ? 3 : 2);
 	SPMV_TRY(warp_geometry(h));
 	int64_t tiles = ceil_div(U, TILE_UNITS);
 	int64_t nch = 0;
@@ -466,7 +598,7 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 		SPMV_TRY(counts.alloc(tiles * sizeof(int64_t), s));
 		SPMV_TRY(offs.alloc((tiles + 1) * sizeof(int64_t), s));
 		unsigned g = (unsigned) ceil_div(tiles, 128);
-		warp_chunks_kernel<false><<<g, 128, 0, s>>>(d_P, U, V, h.block_cap, counts.as<int64_t>(), nullptr, nullptr);
+		warp_chunks_kernel<false><<<g, 128, 0, s>>>(d_P, U, V, gran, h.block_cap, counts.as<int64_t>(), nullptr, nullptr);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		SPMV_TRY(scan_exclusive(counts.as<int64_t>(), offs.as<int64_t>(), tiles, s));
 		SPMV_CUDA_TRY(cudaMemcpyAsync(&nch, offs.as<int64_t>() + tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -476,7 +608,7 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 			return SPMV_ERR_OVERFLOW;
 		}
 		SPMV_TRY(h.alloc(&h.d_chunks, nch));
-		warp_chunks_kernel<true><<<g, 128, 0, s>>>(d_P, U, V, h.block_cap, nullptr, offs.as<int64_t>(), h.d_chunks);
+		warp_chunks_kernel<true><<<g, 128, 0, s>>>(d_P, U, V, gran, h.block_cap, nullptr, offs.as<int64_t>(), h.d_chunks);
 		SPMV_CUDA_TRY(cudaGetLastError());
 	}
 	h.num_chunks = nch;
@@ -536,6 +668,8 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.V = h.desc.vec_len;
 		a.ymap = (fmt == SPMV_FMT_SELL_SORTED) ? h.d_rev : nullptr;
 	}
+	if (h.exec_kernel == 9)
+		a.cols = h.d_tcols;
 	WarpFn kern = pick_warp(h);
 	kern<<<h.grid, WARP_CTA_THREADS, h.smem_bytes, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());

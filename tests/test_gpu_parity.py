@@ -194,29 +194,34 @@ def _sliced_ref(orc, g, fmt, C):
     return orc.sell_sorted_spmv(orc.sell_sorted_convert(rp, ci, v, C, T), m, C, x)
 
 
-@pytest.mark.parametrize("fmt,C", [("sell_c_s", 32), ("sell_c_s", 64), ("sell", 8), ("sell_sorted", 16)])
-@pytest.mark.parametrize("threads,block_rows,tiles,stages", [(0, 0, 0, 0), (96, 64, 1, 2), (256, 128, 3, 3),
-                                                             (512, 256, 8, 4)])
-def test_tiled_kernel_matches_reference(sb, orc, fmt, C, threads, block_rows, tiles, stages):
-    """Kernel 8 (kernel 4 over the column indices in row-major 8-column tiles): same y bits
-    as the reference SELL order for every golden case, slice heights 8..64 (SELL-C-sigma
-    takes C in [32, 256]); one-tile blocks
+@pytest.mark.parametrize("fmt,C", [("sell_c_s", 32), ("sell_c_s", 64), ("sell", 8), ("sell_sorted", 16),
+                                   ("sell", 32), ("sell_sorted", 32)])
+@pytest.mark.parametrize("kernel,threads,block_rows,tiles,stages", [(8, 0, 0, 0, 0), (8, 96, 64, 1, 2), (8, 256, 128, 3, 3),
+                                                                    (8, 512, 256, 8, 4), (9, 0, 0, 0, 0), (9, 0, 0, 1, 2),
+                                                                    (9, 0, 0, 3, 4)])
+def test_tiled_kernel_matches_reference(sb, orc, fmt, C, kernel, threads, block_rows, tiles, stages):
+    """Kernel 8 (kernel 4 over the column indices in row-major 8-column tiles) and kernel 9
+    (warp-owned slices over the same tiles, x transposed between lanes; slices of 32 rows,
+    other heights fall back to kernel 8): same y bits as the reference SELL order for every
+    golden case, slice heights 8..64 (SELL-C-sigma takes C in [32, 256]); one-tile blocks
     force long slices through chunk runs.  The exported arrays keep the reference layout."""
     kw = dict(sellcs_c=C, sellcs_sigma=512) if fmt == "sell_c_s" else dict(vec_len=C, num_threads=T)
     if threads:
-        kw.update(threads=threads, block_rows=block_rows, block_nnz=tiles * 8 * C, stages=stages)
+        kw.update(threads=threads, block_rows=block_rows)
+    if tiles:
+        kw.update(block_nnz=tiles * 8 * C, stages=stages)
     for name in golden_names():
         g = load_golden(name)
-        mf = _mk(sb, g, fmt, kernel=8, **kw)
+        mf = _mk(sb, g, fmt, kernel=kernel, **kw)
         y = mf.spmv(g["x"], np.full(mf.m, 1.0))
-        assert _eq_bits(y, _sliced_ref(orc, g, fmt, C)).size == 0, (name, fmt, C, threads, tiles, stages)
+        assert _eq_bits(y, _sliced_ref(orc, g, fmt, C)).size == 0, (name, fmt, C, kernel, threads, tiles, stages)
         if fmt == "sell_c_s" and name == golden_names()[0]:
             arr = orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], C, 512)
             assert np.array_equal(mf.export("column_indices"), arr["column_indices"])
 
 
 def test_tiled_kernel_long_slices(sb, orc):
-    """Kernel 8 on a skewed matrix (rows up to 3000 entries among rows of 0-40, empty rows):
+    """Kernels 8 and 9 on a skewed matrix (rows up to 3000 entries among rows of 0-40, empty rows):
     slices wider than a block run as chunks of whole tiles, narrower last tiles included."""
     rng = np.random.default_rng(8)
     m = n = 20000
@@ -230,10 +235,11 @@ def test_tiled_kernel_long_slices(sb, orc):
     g = dict(row_ptr=rp, col_ind=ci, values=v, x=x, n=n)
     for C in (32, 64):
         ref = orc.sellcs_spmv(orc.sellcs_convert(rp, ci, v, C, 512), m, C, x)
-        for kw in [dict(), dict(block_nnz=8 * C, stages=2), dict(block_nnz=24 * C + 8)]:
-            mf = _mk(sb, g, "sell_c_s", kernel=8, sellcs_c=C, sellcs_sigma=512, **kw)
-            y = mf.spmv(x, np.full(m, 1.0))
-            assert _eq_bits(y, ref).size == 0, (C, kw)
+        for kernel in (8, 9):
+            for kw in [dict(), dict(block_nnz=8 * C, stages=2), dict(block_nnz=24 * C + 8)]:
+                mf = _mk(sb, g, "sell_c_s", kernel=kernel, sellcs_c=C, sellcs_sigma=512, **kw)
+                y = mf.spmv(x, np.full(m, 1.0))
+                assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
 def test_tiled_kernel_rejects_small_blocks(sb):
