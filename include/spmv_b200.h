@@ -78,8 +78,7 @@ extern "C" {
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
  *                    threads per CTA), 0 = default.
- *   kernel          -1: the format's default (4 for csr_naive, 8 for SELL-C-sigma, 0
- *                       otherwise);
+ *   kernel          -1: the format's default (8 for SELL-C-sigma, 4 for the others);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
  *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);

@@ -454,9 +454,9 @@ static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
 	return SPMV_OK;
 }
 
-// Kernel choice: -1 = the format's default (the warp-specialised kernel for csr_naive, the
-// warp-autonomous own-gather kernel for SELL-C-sigma with C <= 32, the CTA staged kernel
-// otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
+// Kernel choice: -1 = the format's default (the tiled warp-specialised kernel for
+// SELL-C-sigma, the warp-specialised kernel otherwise: the fastest of each on the 4M-row
+// configuration); 0 = CTA
 // staged kernel; 1 = direct column-major kernel (slices of >= 32 rows only); 2 =
 // warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
 // block's gather overlapping this block's rows; 4 = warp-specialised staged kernel; 5 = CTA
@@ -469,11 +469,15 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
 	if (k < 0) {
-		if (h.desc.format == SPMV_FMT_CSR_NAIVE)
-			k = 4;
-		else if (h.desc.format == SPMV_FMT_SELL_C_S)
-			k = 8;
-		else
+		// measured on the 4M-row matrix: kernel 4 is the fastest for csr_naive (0.196-0.207 ms),
+		// csr_vec (0.344 against kernel 0's 0.391), sell (0.319 / 0.354) and sell_sorted
+		// (0.341 / 0.371); kernel 8 for SELL-C-sigma (0.255-0.264)
+		k = h.desc.format == SPMV_FMT_SELL_C_S ? 8 : 4;
+		// a requested staging block too large for their two-stage pipeline (about 220 KB of
+		// shared memory per CTA at 12, 20 or 21 bytes an entry) goes to the CTA staged kernel,
+		// which stages fewer blocks at once
+		const int per = k == 8 ? 21 : (h.desc.format == SPMV_FMT_CSR_NAIVE ? 12 : 20);
+		if (h.desc.block_nnz > 0 && 2 * ((int64_t) h.desc.block_nnz + 16) * per > 220 * 1024 - 256)
 			k = 0;
 	}
 	if (k == 1 && V < 32)
