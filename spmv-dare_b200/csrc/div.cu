@@ -675,17 +675,18 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 	const int lane = threadIdx.x % L;
 	const int cidx = threadIdx.x / L;
 	const bool active = cidx < tpl;
-	int64_t kstart = 0, cstart = 0;
-	for (int64_t g = 0; g < nrf; g++) {
-		const int64_t rf = ld_u32(rfs + 4 * g), u = ld_u32(nus + 4 * g);
-		const int64_t dv = u / L, md = u % L;
-		const int64_t n_i = dv + (lane < md ? 1 : 0);          // positions of this lane
-		const int64_t per = (n_i + tpl - 1) / tpl;
-		const int64_t p0 = active ? (int64_t) cidx * per : 0;
-		const int64_t p1 = active ? min(n_i, p0 + per) : 0;
+	// packet-local counts and offsets fit in 32 bits (a packet holds at most 2^31 values and bytes)
+	int kstart = 0, cstart = 0;
+	for (int g = 0; g < (int) nrf; g++) {
+		const int rf = (int) ld_u32(rfs + 4 * g), u = (int) ld_u32(nus + 4 * g);
+		const int dv = u / L, md = u % L;
+		const int n_i = dv + (lane < md ? 1 : 0);          // positions of this lane
+		const int per = (n_i + tpl - 1) / tpl;
+		const int p0 = active ? cidx * per : 0;
+		const int p1 = active ? min(n_i, p0 + per) : 0;
 		// 1) payload bytes of this chunk
-		int64_t nbytes = 0;
-		for (int64_t pos = p0; pos < p1; pos++)
+		int nbytes = 0;
+		for (int pos = p0; pos < p1; pos++)
 			nbytes += codes[kstart + pos * L + lane] & 15;
 		scan_i[threadIdx.x] = nbytes;
 		__syncthreads();
@@ -699,12 +700,12 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 			lane_cursor[lane] = run;      // next group continues the lane stream
 		}
 		__syncthreads();
-		const int64_t bstart = scan_i[threadIdx.x];
+		const int bstart = (int) scan_i[threadIdx.x];
 		// 2) value difference sum of this chunk
 		uint64_t dsum = 0;
 		{
-			int64_t b = bstart;
-			for (int64_t pos = p0; pos < p1; pos++) {
+			int b = bstart;
+			for (int pos = p0; pos < p1; pos++) {
 				const uint8_t code = codes[kstart + pos * L + lane];
 				const int len = code & 15, tz = (code >> 2) & ~3;
 				dsum += ld_bytes(lanes + b, len) << tz;
@@ -724,17 +725,44 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 		}
 		__syncthreads();
 		// 3) values, coordinates, products
-		{
+		if (rf == 1) {
+			// one coordinate per value (k = pos * L + lane): decode 4 positions, issue their x
+			// loads together, then add the products in the same order
 			uint64_t val = scan_u[threadIdx.x];
-			int64_t b = bstart;
-			for (int64_t pos = p0; pos < p1; pos++) {
+			int b = bstart;
+			for (int pos0 = p0; pos0 < p1; pos0 += 4) {
+				double vv[4], xv[4];
+				int rr[4];
+				#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					const int pos = pos0 + q;
+					if (pos < p1) {
+						const uint8_t code = codes[kstart + pos * L + lane];
+						const int len = code & 15, tz = (code >> 2) & ~3;
+						val += ld_bytes(lanes + b, len) << tz;
+						b += len;
+						vv[q] = __longlong_as_double((long long) val);
+						const uint64_t c = ld_bytes(coords + (cstart + pos * L + lane) * cb, cb);
+						rr[q] = (int) (c & rmask);
+						xv[q] = __ldg(a.x + col_min + (int64_t) ((c >> row_bits) & cmask));
+					}
+				}
+				#pragma unroll
+				for (int q = 0; q < 4; q++)
+					if (pos0 + q < p1)
+						atomicAdd(&ys[rr[q]], vv[q] * xv[q]);
+			}
+		} else {
+			uint64_t val = scan_u[threadIdx.x];
+			int b = bstart;
+			for (int pos = p0; pos < p1; pos++) {
 				const uint8_t code = codes[kstart + pos * L + lane];
 				const int len = code & 15, tz = (code >> 2) & ~3;
 				val += ld_bytes(lanes + b, len) << tz;
 				b += len;
 				const double vd = __longlong_as_double((long long) val);
-				for (int64_t j = 0; j < rf; j++) {
-					const int64_t k = (pos < dv) ? (pos * L) * rf + L * j + lane : (dv * L + lane) * rf + j;
+				for (int j = 0; j < rf; j++) {
+					const int k = (pos < dv) ? (pos * L) * rf + L * j + lane : (dv * L + lane) * rf + j;
 					const uint64_t c = ld_bytes(coords + (cstart + k) * cb, cb);
 					const int64_t rr = (int64_t) (c & rmask);
 					const int64_t cc = (int64_t) ((c >> row_bits) & cmask);
