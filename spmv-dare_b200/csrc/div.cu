@@ -623,6 +623,39 @@ struct DivArgs {
 	double * y;
 };
 
+// Exclusive scan over the threads of each lane (thread t: lane t % L, position t / L in its
+// lane), in position order: the sum of v over the lane's earlier threads.  L is a power of two
+// and DEC_THREADS threads take part.  Below 32 lanes a warp holds 32 / L threads of each lane,
+// scanned with shuffles (strides L, 2L, ...), then the 8 warp totals of the lane are added from
+// shared memory; from 32 lanes up a lane has at most 8 threads, one per warp, added directly.
+// vals and wsum are DEC_THREADS-entry shared arrays; one barrier inside.
+template <typename T>
+__device__ __forceinline__ T lane_exclusive_scan(T v, int L, T * vals, T * wsum)
+{
+	const int t = threadIdx.x, lane = t % L, w = t >> 5, wl = t & 31;
+	vals[t] = v;
+	T inc = v;
+	if (L < 32) {
+		for (int d = L; d < 32; d <<= 1) {
+			const T o = __shfl_up_sync(0xffffffffu, inc, d);
+			if (wl >= d)
+				inc += o;
+		}
+		if (wl >= 32 - L)
+			wsum[w * L + (wl - (32 - L))] = inc;     // the warp's total of this lane
+	}
+	__syncthreads();
+	T pre = inc - v;
+	if (L < 32) {
+		for (int q = 0; q < w; q++)
+			pre += wsum[q * L + lane];
+	} else {
+		for (int c = 0; c < t / L; c++)
+			pre += vals[c * L + lane];
+	}
+	return pre;
+}
+
 // One CTA per packet.  The decoder reads the packet byte by byte, threads far apart, so the
 // packet is first copied into shared memory with 16-byte loads (the stream is padded by 16
 // bytes and 256-byte aligned, so the rounded copy stays inside it) and decoded from there
@@ -634,6 +667,8 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 	__shared__ int64_t scan_i[DEC_THREADS];
 	__shared__ uint64_t scan_u[DEC_THREADS];
 	__shared__ int64_t lane_cursor[DEC_THREADS];
+	__shared__ int64_t wsum_i[DEC_THREADS];
+	__shared__ uint64_t wsum_u[DEC_THREADS];
 	const int64_t p = blockIdx.x;
 	const int64_t off = a.pkt_off[p], pend = a.pkt_off[p + 1];
 	const uint8_t * h = a.data + off;
@@ -688,19 +723,10 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 		int nbytes = 0;
 		for (int pos = p0; pos < p1; pos++)
 			nbytes += codes[kstart + pos * L + lane] & 15;
-		scan_i[threadIdx.x] = nbytes;
-		__syncthreads();
-		if (active && cidx == 0) {
-			int64_t run = lane_cursor[lane];
-			for (int c = 0; c < tpl; c++) {
-				const int64_t t = scan_i[c * L + lane];
-				scan_i[c * L + lane] = run;
-				run += t;
-			}
-			lane_cursor[lane] = run;      // next group continues the lane stream
-		}
-		__syncthreads();
-		const int bstart = (int) scan_i[threadIdx.x];
+		const int bstart = (int) (lane_cursor[lane] + lane_exclusive_scan<int64_t>(nbytes, L, scan_i, wsum_i));
+		__syncthreads();                 // every thread has read its lane's cursor
+		if (active && cidx == tpl - 1)
+			lane_cursor[lane] = bstart + nbytes;     // next group continues the lane stream
 		// 2) value difference sum of this chunk
 		uint64_t dsum = 0;
 		{
@@ -712,23 +738,12 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 				b += len;
 			}
 		}
-		__syncthreads();
-		scan_u[threadIdx.x] = dsum;
-		__syncthreads();
-		if (active && cidx == 0) {
-			uint64_t run = 0;       // every lane restarts at 0 in each group
-			for (int c = 0; c < tpl; c++) {
-				const uint64_t t = scan_u[c * L + lane];
-				scan_u[c * L + lane] = run;
-				run += t;
-			}
-		}
-		__syncthreads();
+		const uint64_t dstart = lane_exclusive_scan<uint64_t>(dsum, L, scan_u, wsum_u);   // lanes restart at 0
 		// 3) values, coordinates, products
 		if (rf == 1) {
 			// one coordinate per value (k = pos * L + lane): decode 4 positions, issue their x
 			// loads together, then add the products in the same order
-			uint64_t val = scan_u[threadIdx.x];
+			uint64_t val = dstart;
 			int b = bstart;
 			for (int pos0 = p0; pos0 < p1; pos0 += 4) {
 				double vv[4], xv[4];
@@ -753,7 +768,7 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 						atomicAdd(&ys[rr[q]], vv[q] * xv[q]);
 			}
 		} else {
-			uint64_t val = scan_u[threadIdx.x];
+			uint64_t val = dstart;
 			int b = bstart;
 			for (int pos = p0; pos < p1; pos++) {
 				const uint8_t code = codes[kstart + pos * L + lane];
