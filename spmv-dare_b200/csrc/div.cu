@@ -592,11 +592,9 @@ __global__ void split_rows_kernel(const int32_t * split_flag, const int64_t * ex
 // ------------------------------------------------------------------ decoder + SpMV
 constexpr int DEC_THREADS = 256;
 constexpr int DEC_MAX_ROWS = 256;
-constexpr int64_t DIV_STAGE_MAX = 96 * 1024;   // largest packet copied to shared memory
 
 // n <= 8 little-endian bytes at an unaligned address: two aligned 8-byte loads and a funnel
-// shift.  The reads reach at most 15 bytes past p; the stream is padded by 16 bytes and the
-// shared packet copy holds 15 bytes of slack past its packet.
+// shift.  The reads reach at most 15 bytes past p; the stream is padded by 16 bytes.
 __device__ __forceinline__ uint64_t ld_bytes(const uint8_t * p, int n)
 {
 	const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -618,7 +616,6 @@ struct DivArgs {
 	const int4 * meta;
 	int64_t npackets;
 	int L;
-	int stage;                 // bytes of the CTA's shared copy of its packet (0: decode from HBM)
 	const double * x;
 	double * y;
 };
@@ -656,13 +653,11 @@ __device__ __forceinline__ T lane_exclusive_scan(T v, int L, T * vals, T * wsum)
 	return pre;
 }
 
-// One CTA per packet.  The decoder reads the packet byte by byte, threads far apart, so the
-// packet is first copied into shared memory with 16-byte loads (the stream is padded by 16
-// bytes and 256-byte aligned, so the rounded copy stays inside it) and decoded from there
-// through a generic pointer; packets larger than the copy budget are decoded from HBM.
+// One CTA per packet, at most 85 registers a thread so that 3 CTAs share an SM.  (Copying the
+// packet into shared memory first was measured slower: the copy's shared memory leaves 2 CTAs
+// an SM, and the byte reads conflict on the banks.)
 __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 {
-	extern __shared__ __align__(16) uint8_t pk[];
 	__shared__ double ys[DEC_MAX_ROWS];
 	__shared__ int64_t scan_i[DEC_THREADS];
 	__shared__ uint64_t scan_u[DEC_THREADS];
@@ -670,18 +665,7 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 	__shared__ int64_t wsum_i[DEC_THREADS];
 	__shared__ uint64_t wsum_u[DEC_THREADS];
 	const int64_t p = blockIdx.x;
-	const int64_t off = a.pkt_off[p], pend = a.pkt_off[p + 1];
-	const uint8_t * h = a.data + off;
-	if (a.stage > 0 && pend - (off & ~(int64_t) 15) + 15 <= a.stage) {
-		const int64_t base = off & ~(int64_t) 15;
-		const int n16 = (int) ((pend - base + 15) >> 4);
-		const uint4 * src = reinterpret_cast<const uint4 *>(a.data + base);
-		uint4 * dst = reinterpret_cast<uint4 *>(pk);
-		for (int i = threadIdx.x; i < n16; i += blockDim.x)
-			dst[i] = __ldg(src + i);
-		__syncthreads();
-		h = pk + (off - base);
-	}
+	const uint8_t * h = a.data + a.pkt_off[p];
 	const int L = a.L;
 	const int64_t nv = ld_u32(h + 0), nu = ld_u32(h + 4), nrows = ld_u32(h + 8);
 	const int64_t row_min = ld_u32(h + 12), col_min = ld_u32(h + 16);
@@ -1025,18 +1009,7 @@ int convert_div(Handle & h)
 	SPMV_CUDA_TRY(cudaMemcpyAsync(&total, h.d_pkt + NP, 8, cudaMemcpyDeviceToHost, s));
 	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
 	h.div_bytes = total;
-	SPMV_TRY(h.alloc(&h.d_div, total + 16));
-	{
-		// the largest packet sets the decoder's shared copy (none above DIV_STAGE_MAX)
-		std::vector<int64_t> off((size_t) NP + 1);
-		SPMV_CUDA_TRY(cudaMemcpyAsync(off.data(), h.d_pkt, (NP + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-		SPMV_CUDA_TRY(cudaStreamSynchronize(s));
-		int64_t mx = 0;
-		for (int64_t i = 0; i < NP; i++)
-			mx = off[(size_t) i + 1] - off[(size_t) i] > mx ? off[(size_t) i + 1] - off[(size_t) i] : mx;
-		const int64_t need = ((mx + 31) / 16) * 16;
-		h.div_stage = need <= DIV_STAGE_MAX ? (int) need : 0;
-	}
+	SPMV_TRY(h.alloc(&h.d_div, total + 16));     // 16 bytes of pad: the decoder reads whole words
 
 	// 8) scatter the bytes
 	header_kernel<<<(unsigned) ceil_div(NP, 128), 128, 0, s>>>(h.d_pkt, pk_g0.as<int32_t>(), pk_nv.as<int32_t>(),
@@ -1125,12 +1098,9 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.meta = h.d_pkt_meta;
 	a.npackets = h.num_packets;
 	a.L = h.desc.vec_len;
-	a.stage = h.div_stage;
 	a.x = d_x;
 	a.y = d_y;
-	if (h.div_stage > 48 * 1024)
-		SPMV_CUDA_TRY(cudaFuncSetAttribute(div_spmv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, h.div_stage));
-	div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, (size_t) h.div_stage, s>>>(a);
+	div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;
 }

@@ -147,7 +147,6 @@ struct Handle {
 	double * d_split_part = nullptr;    // partial sums of rows split across packets
 	int32_t * d_split_rows = nullptr;
 	int64_t num_split = 0;
-	int div_stage = 0;                  // bytes of the decoder's shared packet copy (0: none)
 
 	// host-buffer path staging
 	double * d_x = nullptr;
