@@ -73,7 +73,7 @@ extern "C" {
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,
- *                        kernel 4 always sums in order).                           default 1
+ *                        the others always sum in order).                          default 1
  *   values               SPMV_VALUES_F64 or SPMV_VALUES_F32.                       default F64
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
