@@ -474,9 +474,9 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		// (0.341 / 0.371); kernel 8 for SELL-C-sigma (0.255-0.264)
 		k = h.desc.format == SPMV_FMT_SELL_C_S ? 8 : 4;
 		// a requested staging block too large for their two-stage pipeline (about 220 KB of
-		// shared memory per CTA at 12, 20 or 21 bytes an entry) goes to the CTA staged kernel,
+		// shared memory per CTA at 12, 16 or 17 bytes an entry) goes to the CTA staged kernel,
 		// which stages fewer blocks at once
-		const int per = k == 8 ? 21 : (h.desc.format == SPMV_FMT_CSR_NAIVE ? 12 : 20);
+		const int per = k == 8 ? 17 : (h.desc.format == SPMV_FMT_CSR_NAIVE ? 12 : 16);
 		if (h.desc.block_nnz > 0 && 2 * ((int64_t) h.desc.block_nnz + 16) * per > 220 * 1024 - 256)
 			k = 0;
 	}
@@ -503,10 +503,12 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 	if (k == 3 && h.desc.stages == 0)
 		h.stages = 3;
 	if (k == 4) {
-		// defaults measured on the 4M-row matrix: 768-entry blocks, 2 stages, 3 gather warps
-		// and 2 row warps (0.196 ms for csr_naive; 3 stages 0.202 ms)
+		// defaults measured on the 4M-row matrix: 2 stages, 3 gather warps and 2 row warps;
+		// 768-entry blocks for csr_naive (0.195-0.207 ms; 3 stages 0.202 ms), 1280 for the FMA
+		// formats, whose stages take 16 bytes an entry (csr_vec 0.316 ms, sell 0.285 ms; 768-entry
+		// blocks 0.334 / 0.291)
 		if (h.desc.block_nnz == 0)
-			h.block_cap = 768;
+			h.block_cap = h.desc.format == SPMV_FMT_CSR_NAIVE ? 768 : 1280;
 		if (h.desc.stages == 0)
 			h.stages = 2;
 		if (h.desc.threads == 0)

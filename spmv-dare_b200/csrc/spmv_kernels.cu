@@ -45,6 +45,7 @@ struct StagedArgs {
 	int stage_bytes;
 	int exact;
 	int row_threads;         // warp-specialised kernel: threads of the row warps
+	int cols_off;            // warp-specialised kernel: byte offset of the staged columns in a stage
 	const int64_t * ranges;  // warp-specialised kernel: each CTA's contiguous block range
 	int * err;
 };
@@ -742,7 +743,7 @@ __device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock
 	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
 	const uint32_t cnt = (uint32_t) (e1 - e0);
 	double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
-	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cap_al * 8);
+	int32_t * sc = reinterpret_cast<int32_t *>(smem + (size_t) s * a.stage_bytes + (size_t) a.cols_off);
 	fence_proxy_async_smem();
 	mbar_arrive_expect_tx(&bars[s], cnt * 12u);
 	bulk_g2s(sv, a.vals + e0, cnt * 8u, &bars[s]);
@@ -842,8 +843,8 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		const int gt = threadIdx.x;
 		for (int64_t b = b_begin; b < b_end; b++) {
 			const bool ok = mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles);
-			if (!__all_sync(0xffffffffu, ok)) {            // the warp leaves together
-				if ((gt & 31) == 0)
+			if (named_bar_or(2, ng, !ok)) {                // the gather warps leave together
+				if (gt == 0)
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 				return;
 			}
@@ -851,12 +852,17 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 			if (d.elems > 0) {
 				uint8_t * st = smem + (size_t) s * a.stage_bytes;
 				double * sv = reinterpret_cast<double *>(st);
-				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cap_al * 8);
-				double * xg = reinterpret_cast<double *>(st + (size_t) a.cap_al * 12);
+				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cols_off);
+				double * xg = reinterpret_cast<double *>(st + (size_t) a.cap_al * 8);
 				const int off = d.elem0 & 3;
-				// WS_GATHER_SLOTS independent loads in flight per thread: the column loads of a group are
-				// all issued before any store of the group, so the x loads overlap
-				for (int e0 = gt; e0 < d.elems; e0 += WS_GATHER_SLOTS * ng) {
+				// Rounds of WS_GATHER_SLOTS * ng consecutive entries, the same count for every gather
+				// thread; WS_GATHER_SLOTS independent loads in flight per thread.  The FMA formats'
+				// columns sit at the top of the x buffer: x of position p covers column positions
+				// below p + 1 only, so once every gather thread has read the round's columns (named
+				// barrier 2) the round's x overwrites columns already read.
+				const int per_round = WS_GATHER_SLOTS * ng;
+				for (int rb = 0; rb < d.elems; rb += per_round) {
+					const int e0 = rb + gt;
 					double xv[WS_GATHER_SLOTS];
 					#pragma unroll
 					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
@@ -864,6 +870,8 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 						if (e < d.elems)
 							xv[k] = ldg(a.x + sc[off + e]);
 					}
+					if (A != Arith::SEQ_SPLIT)
+						named_bar_sync(2, ng);
 					#pragma unroll
 					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
 						const int e = e0 + k * ng;
@@ -923,10 +931,10 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		uint8_t * st = smem + (size_t) s * a.stage_bytes;
 		if (d.units >= 0)
 			rows_t<K, A, L, YMAP, TX>(a, d, reinterpret_cast<const double *>(st),
-					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), js0, je0, yi, rt, nr);
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 8), js0, je0, yi, rt, nr);
 		else
 			ws_chunk<K, A, L, YMAP, TX>(a, d, reinterpret_cast<const double *>(st),
-					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 12), yi, rt, acc, ln);
+					reinterpret_cast<const double *>(st + (size_t) a.cap_al * 8), yi, rt, acc, ln);
 		named_bar_sync(1, nr);
 		if (rt == 0 && nb < b_end) {
 			sdesc[s] = dnext;
@@ -1185,12 +1193,21 @@ int pipe_stage_bytes(int format, int cap_al)
 	return (int) (ceil_div((int64_t) cap_al * per, 128) * 128);
 }
 
-// Bytes of one stage of the tiled kernel: values, columns and the x buffer (entry e at
-// e + e / 8).
-int tiled_stage_bytes(int cap_al)
+// Stage of the warp-specialised kernels (4 and 8): csr_naive stages values and columns, the
+// rounded products replacing the values (12 bytes an entry); the FMA formats stage values
+// and an x buffer whose top holds the staged columns until the gather overwrites them (16
+// bytes an entry; 17 with the tiled kernel's e + e / 8 buffer).  Returns the stage bytes and
+// the columns' byte offset (a multiple of 16, as the bulk copy needs).
+int ws_stage_layout(int format, int cap_al, bool tiled, int * cols_off)
 {
-	const int64_t xb = (int64_t) cap_al + ceil_div((int64_t) cap_al, 8);
-	return (int) (ceil_div((int64_t) cap_al * 12 + xb * 8, 128) * 128);
+	if (format == SPMV_FMT_CSR_NAIVE) {
+		*cols_off = cap_al * 8;
+		return (int) (ceil_div((int64_t) cap_al * 12, 128) * 128);
+	}
+	const int64_t xb = tiled ? ceil_div(8 * ((int64_t) cap_al + ceil_div((int64_t) cap_al, 8)), 16) * 16
+	                         : (int64_t) cap_al * 8;
+	*cols_off = (int) ((int64_t) cap_al * 8 + xb - (int64_t) cap_al * 4);
+	return (int) (ceil_div((int64_t) cap_al * 8 + xb, 128) * 128);
 }
 
 }  // namespace
@@ -1317,9 +1334,9 @@ int staged_geometry(Handle & h)
 {
 	if (h.exec_kernel == 4 || h.exec_kernel == 8) {
 		const int cap_al = h.block_cap + 8;
-		const int stage_bytes = h.exec_kernel == 8 ? tiled_stage_bytes(cap_al)
-		                        : h.desc.values == SPMV_VALUES_F32 ? f32ws_stage_bytes(cap_al)
-		                        : pipe_stage_bytes(h.desc.format, cap_al);
+		int cols_off = 0;
+		const int stage_bytes = h.desc.values == SPMV_VALUES_F32 ? f32ws_stage_bytes(cap_al)
+		                        : ws_stage_layout(h.desc.format, cap_al, h.exec_kernel == 8, &cols_off);
 		const int max_stages = (220 * 1024 - 128) / stage_bytes;
 		if (max_stages < 2) {
 			set_error(SPMV_ERR_ARG, "warp-specialised kernel: staging block of %d entries exceeds shared memory",
@@ -1501,13 +1518,13 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
 	} else if (h.exec_kernel == 4) {
 		kern = pick_ws(h);
-		a.stage_bytes = pipe_stage_bytes(fmt, a.cap_al);
+		a.stage_bytes = ws_stage_layout(fmt, a.cap_al, false, &a.cols_off);
 		a.row_threads = h.row_threads;
 		a.ranges = h.d_cta_ranges;
 	} else if (h.exec_kernel == 8) {
 		kern = pick_ws_tiled(h);
 		a.cols = h.d_tcols;
-		a.stage_bytes = tiled_stage_bytes(a.cap_al);
+		a.stage_bytes = ws_stage_layout(fmt, a.cap_al, true, &a.cols_off);
 		a.row_threads = h.row_threads;
 		a.ranges = h.d_cta_ranges;
 	}
