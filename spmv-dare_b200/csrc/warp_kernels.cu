@@ -1,4 +1,4 @@
-// Warp-autonomous staged SpMV (the default kernel of the CSR and narrow-SELL formats).
+// Warp-autonomous staged SpMV (kernels 2, 6 and 9; options beside the warp-specialised defaults).
 //
 // Every warp owns a contiguous run of "chunks" of the matrix and its own pipeline in
 // shared memory: a ring of bulk-copy stages (cp.async.bulk global->shared, completion on a
