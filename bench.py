@@ -211,6 +211,32 @@ def generate(sb, args):
     return g.row_ptr, g.col_ind, v, x
 
 
+def make_config(args, fmt, m, n, nnz, B, world):
+    """The `config` object of both arms (same keys, so the two lines compare key by key)."""
+    return {"workload": WORKLOAD if not args.rows else WORKLOAD.replace("4Mx4M", f"{m}x{n}"),
+            "format": fmt, "m": m, "n": n, "nnz": nnz, "bytes_per_spmv": B,
+            "l2": "no flush: inputs (1.05 GB/SpMV) exceed the 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "format_params": FORMAT_PARAMS.get(fmt, {})}
+
+
+def convert_median(sb, rp, ci, v, m, n, nnz, fmt, reps=3, **params):
+    """Converts `reps` times and keeps the handle of the median conversion time; returns
+    (handle, {convert_ms, alloc_ms, copy_in_ms} of that conversion, all conversion times)."""
+    runs = []
+    for _ in range(reps):
+        mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format=fmt, **params)
+        runs.append(mf)
+    runs.sort(key=lambda h: h.convert_ms)
+    keep = runs[len(runs) // 2]
+    allms = sorted(h.convert_ms for h in runs)
+    for h in runs:
+        if h is not keep:
+            h.destroy()
+    return keep, {"convert_ms": keep.convert_ms, "convert_alloc_ms": keep.alloc_ms,
+                  "convert_copy_in_ms": keep.copy_in_ms}, allms
+
+
 def time_device(mf, xd, yd, steps, warmup, torch):
     stream = torch.cuda.current_stream()
     for _ in range(warmup):
@@ -245,7 +271,7 @@ def run_ours(args):
     head = None
     for fmt in formats:
         try:
-            mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format=fmt, **FORMAT_PARAMS.get(fmt, {}))
+            mf, conv, conv_all = convert_median(sb, rp, ci, v, m, n, nnz, fmt, **FORMAT_PARAMS.get(fmt, {}))
         except sb.SpmvError as e:
             per_format[fmt] = {"error": str(e)}
             continue
@@ -263,7 +289,8 @@ def run_ours(args):
         med = statistics.median(per)
         rec = {"ms_per_step": ms, "ms_median": med, "gbs": B * 1e-9 / (ms * 1e-3),
                "gflops": flops * 1e-9 / (ms * 1e-3), "hbm_frac": B * 1e-9 / (med * 1e-3) / peak,
-               "convert_ms": mf.convert_ms, "mem_footprint": mf.mem_footprint, "stored_elems": mf.stored_elems,
+               **conv, "convert_ms_all": [round(t, 2) for t in conv_all],
+               "mem_footprint": mf.mem_footprint, "stored_elems": mf.stored_elems,
                "kernels_per_spmv": mf.kernels_per_run}
         per_format[fmt] = rec
         if fmt == args.format:
@@ -306,12 +333,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (the reference's artificial generator restated natively, config 2; values 2v-1, x U[-1,1))",
-        "config": {"workload": WORKLOAD if not args.rows else WORKLOAD.replace("4Mx4M", f"{m}x{n}"),
-                   "format": args.format, "m": m, "n": n, "nnz": nnz,
-                   "bytes_per_spmv": B, "gflops": round(head["gflops"], 2),
-                   "l2": "no flush: inputs (1.05 GB/SpMV) exceed the 126 MB L2",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "format_params": FORMAT_PARAMS.get(args.format, {})},
+        "config": make_config(args, args.format, m, n, nnz, B, world),
+        "gflops": round(head["gflops"], 2),
         "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_s * 1e3, 4)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -323,6 +346,11 @@ def run_ours(args):
         "per_format": {k: {kk: (float(f"{vv:.5g}") if isinstance(vv, float) else vv) for kk, vv in r.items()}
                        for k, r in per_format.items()},
     }
+    if args.all_formats and not args.no_batch:
+        del head, mf
+        torch.cuda.empty_cache()
+        out["batch"] = batch_block(sb, torch, dev, args, world, peak)
+        torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with stdout_to_stderr():
             out["cpu_baseline"] = cpu_baseline(args.format, rp, ci, v, x, B, sample_s=args.cpu_seconds)
@@ -332,6 +360,58 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def batch_block(sb, torch, dev, args, world, peak):
+    """The 512-matrix batch (C4) inside the default line: the autotuned batch (every matrix
+    csr_naive with these kernels: one block-diagonal SpMV, CUDA-graph replay) and the same
+    matrices with formats dealt round robin over csr_naive / sell / sell_sorted / sell_c_s,
+    which runs the persistent work-queue kernel; y of each against the matrices' own
+    handles, bit for bit."""
+    from spmv_dare_b200 import tuning
+
+    mats, classes, xs, B = batch_matrices(sb, args.batch_count, False)
+    xh = np.concatenate(xs)
+    xd = torch.from_numpy(xh).to(dev)
+    out = {"workload": BATCH_WORKLOAD, "matrices": len(mats), "bytes_per_step": B,
+           "nnz_total": sum(int(mt[0][-1]) for mt in mats)}
+    steps = max(5, args.steps // 2)
+    mixed_pool = [tuning.CLASSES.index({"format": "sell", "vec_len": 4}),
+                  tuning.CLASSES.index({"format": "sell_sorted", "vec_len": 4}),
+                  tuning.CLASSES.index({"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 0}),
+                  0]
+    legs = [("tuned", classes), ("mixed", [mixed_pool[i % 4] for i in range(len(mats))])]
+    for name, cls in legs:
+        batch = sb.Batch(mats, [tuning.batch_desc(c) for c in cls])
+        yd = torch.empty(batch.total_y, dtype=torch.float64, device=dev)
+        barrier(world)
+        ms, per = time_events(lambda: batch.spmv(xd, yd, graph=True), steps, args.warmup, torch)
+        barrier(world)
+        ms = max_over_ranks(world, ms)
+        y_batch = yd.cpu().numpy().copy()
+        # the same matrices, each through its own handle of the same format
+        ident = True
+        for i, ((rp, ci, v, m, n), c) in enumerate(zip(mats, cls)):
+            h = sb.csr_to_format(rp, ci, v, m, n, int(rp[-1]), **tuning.batch_desc(c))
+            xo, yo = int(batch.x_offsets[i]), int(batch.y_offsets[i])
+            yv = torch.empty(m, dtype=torch.float64, device=dev)
+            h.spmv(xd[xo:xo + n], yv)
+            ident = ident and bool(np.array_equal(yv.cpu().numpy().view(np.uint64),
+                                                  y_batch[yo:yo + m].view(np.uint64)))
+            h.destroy()
+        med = statistics.median(per)
+        counts = {}
+        for c in cls:
+            counts[tuning.class_name(c)] = counts.get(tuning.class_name(c), 0) + 1
+        out[name] = {"graph_ms": round(ms, 4), "gbs": round(world * B * 1e-9 / (ms * 1e-3), 1),
+                     "hbm_frac": round(B * 1e-9 / (med * 1e-3) / peak, 4), "formats": counts,
+                     "path": "block-diagonal csr_naive SpMV (warp-specialised kernel)" if batch.num_blocks == 0 or
+                     all(tuning.CLASSES[c]["format"] == "csr_naive" for c in cls) else "persistent work-queue batch_kernel",
+                     "y_identical_to_per_matrix": ident, "steps": steps}
+        batch.destroy()
+        del yd
+        torch.cuda.empty_cache()
+    return out
 
 
 def fp32_variant(sb, torch, dev, rp, ci, v, x, args, per_format):
@@ -430,7 +510,7 @@ def run_reference(args):
         "value": round(val, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (the reference's own generator, config 2; values 2v-1, x U[-1,1))",
-        "config": {"workload": WORKLOAD, "format": name, "m": m, "n": n, "nnz": nnz, "bytes_per_spmv": B},
+        "config": make_config(args, name, m, n, nnz, B, world),
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
                          "sample": f"config 2 full matrix, {args.steps} timed SpMV steps after {args.warmup} warm-up"},
@@ -675,6 +755,7 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "batch"])
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--retune", action="store_true", help="batch: re-run the autotuner instead of its database")
+    ap.add_argument("--no-batch", action="store_true", help="leave the batch block out of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

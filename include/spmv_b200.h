@@ -78,6 +78,14 @@ extern "C" {
  *   block_nnz, block_rows, stages, ctas_per_sm, threads: kernel tuning knobs (entries
  *                    staged per block, rows per block, pipeline depth, CTAs per SM,
  *                    threads per CTA), 0 = default.
+ *   wait_limit_us    bound of every device-side wait (a bulk copy landing, a stage hand-off):
+ *                    a kernel whose wait runs out records SPMV_ERR_TIMEOUT (reported by the
+ *                    next spmv_sync() / spmv_run()), waits for its own copies in flight and
+ *                    leaves.  0 = about 2 s.                                   default 0
+ *   debug_flags      SPMV_DEBUG_WITHHOLD_HANDOFF: the gather warps of the warp-specialised
+ *                    kernels (4, 8 and the FP32 default) never hand a stage to the row
+ *                    warps, so the row warps' wait runs out: a test of the timeout path
+ *                    that faults nothing.                                      default 0
  *   kernel          -1: the format's default (8 for SELL-C-sigma, 4 for the others);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
@@ -118,8 +126,12 @@ typedef struct spmv_format_desc {
 	int32_t ctas_per_sm;
 	int32_t kernel;
 	int32_t threads;
-	int32_t reserved[6];
+	int32_t wait_limit_us;
+	int32_t debug_flags;
+	int32_t reserved[4];
 } spmv_format_desc;
+
+#define SPMV_DEBUG_WITHHOLD_HANDOFF 1
 
 typedef struct spmv_handle spmv_handle;
 
@@ -134,6 +146,8 @@ typedef struct spmv_info {
 	int32_t kernels_per_run;     /* kernel launches one spmv_run_device() makes                  */
 	int32_t format;
 	char    format_name[64];     /* the reference's format_name, e.g. "Naive_CSR_CPU" -> "Naive_CSR_GPU" */
+	double  alloc_ms;            /* part of convert_ms spent in cudaMalloc                         */
+	double  copy_in_ms;          /* part of convert_ms spent copying the CSR arrays to the device  */
 } spmv_info;
 
 /* Fill *desc with the defaults above for `format`. */
@@ -171,9 +185,10 @@ int spmv_run_f32(spmv_handle * h, const float * x, float * y);
 
 /*
  * Allocation-free FP32-storage SpMV with FP64 vectors on the device.  No counterpart in
- * the reference.  For callers that must not allocate device memory during a run: code
- * whose device memory comes from a fixed pool or an arena it does not own, or a call made
- * while a stream is being captured into a CUDA graph, where cudaMalloc is not allowed.
+ * the reference.  For callers that cannot call cudaMalloc while they run: a host program
+ * that owns all device memory through its own pool or arena and gives libraries none of
+ * their own, or a loop with a deadline that cannot take the device-wide synchronisation a
+ * cudaMalloc / cudaFree may cause.
  * Does what spmv_run() does with an FP32 handle and FP64 buffers (x rounded to FP32 once,
  * the Dot2-compensated FP32 SpMV, y widened to FP64), but on device vectors, enqueued on
  * `stream` (NULL: the handle's stream), and with its two temporaries (the FP32 x and the
@@ -181,8 +196,11 @@ int spmv_run_f32(spmv_handle * h, const float * x, float * y);
  * it, for as long as the process lives.
  *   - Limit: n + m <= SPMV_NOALLOC_MAX_ELEMS (262144 FP32 elements, 1 MiB); larger
  *     matrices get SPMV_ERR_ARG and nothing is launched.
+ *   - The handle's device must be the current device (SPMV_ERR_ARG otherwise).
  *   - The first call on a device looks the array's device address up (once per device,
- *     with that device current): make that first call before capturing a stream.
+ *     with that device current): make that first call before any stream capture.  The
+ *     address is not looked up again after a cudaDeviceReset(): do not use the entry point
+ *     across one.
  *   - All calls on a device share the array, and it keeps what the last call wrote.  Every
  *     element a call reads it first writes, so nothing has to start at zero.  Calls whose
  *     executions overlap on the GPU (other streams, other host threads) race on it:

@@ -120,6 +120,8 @@ class Matrix_Format:
         self.stored_elems = int(info.stored_elems)
         self.device_bytes = int(info.device_bytes)
         self.convert_ms = float(info.convert_ms)
+        self.alloc_ms = float(info.alloc_ms)
+        self.copy_in_ms = float(info.copy_in_ms)
         self.kernels_per_run = int(info.kernels_per_run)
         self.num_loops = 0
 

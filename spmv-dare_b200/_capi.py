@@ -53,7 +53,7 @@ class FormatDesc(ctypes.Structure):
         ("sellcs_sigma", c_int32), ("div_packet_vals", c_int32), ("div_tolerance", c_double),
         ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
         ("stages", c_int32), ("ctas_per_sm", c_int32), ("kernel", c_int32), ("threads", c_int32),
-        ("reserved", c_int32 * 6),
+        ("wait_limit_us", c_int32), ("debug_flags", c_int32), ("reserved", c_int32 * 4),
     ]
 
 
@@ -62,7 +62,7 @@ class Info(ctypes.Structure):
         ("m", c_int64), ("n", c_int64), ("nnz", c_int64), ("mem_footprint", c_double),
         ("csr_mem_footprint", c_double), ("stored_elems", c_int64), ("device_bytes", c_int64),
         ("convert_ms", c_double), ("kernels_per_run", c_int32), ("format", c_int32),
-        ("format_name", c_char * 64),
+        ("format_name", c_char * 64), ("alloc_ms", c_double), ("copy_in_ms", c_double),
     ]
 
 

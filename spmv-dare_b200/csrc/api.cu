@@ -77,6 +77,14 @@ static int check_desc(const spmv_format_desc & d)
 			return SPMV_ERR_ARG;
 		}
 	}
+	if (d.wait_limit_us < 0 || d.wait_limit_us > 60000000) {
+		set_error(SPMV_ERR_ARG, "wait_limit_us must be in [0, 60e6] (got %d)", d.wait_limit_us);
+		return SPMV_ERR_ARG;
+	}
+	if (d.debug_flags & ~SPMV_DEBUG_WITHHOLD_HANDOFF) {
+		set_error(SPMV_ERR_ARG, "unknown debug_flags bits 0x%x", d.debug_flags);
+		return SPMV_ERR_ARG;
+	}
 	if (d.values != SPMV_VALUES_F64 && d.values != SPMV_VALUES_F32) {
 		set_error(SPMV_ERR_ARG, "values must be SPMV_VALUES_F64 or SPMV_VALUES_F32");
 		return SPMV_ERR_ARG;
@@ -217,6 +225,7 @@ static int create_common(Handle & h, const int32_t * rp, const int32_t * ci, con
 	SPMV_TRY(h.alloc(&h.d_v, nnz + SPMV_ENTRY_PAD));
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_ci + nnz, 0, SPMV_ENTRY_PAD * sizeof(int32_t), s));
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_v + nnz, 0, SPMV_ENTRY_PAD * sizeof(double), s));
+	const auto tc = std::chrono::steady_clock::now();
 	if (host) {
 		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_rp, rp, (m + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 		if (nnz > 0) {
@@ -237,6 +246,8 @@ static int create_common(Handle & h, const int32_t * rp, const int32_t * ci, con
 			SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_v, v, nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
 		}
 	}
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	h.copy_in_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc).count();
 	SPMV_TRY(convert_all(h));
 	auto t1 = std::chrono::steady_clock::now();
 	h.convert_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -471,6 +482,8 @@ int spmv_get_info(const spmv_handle * H, spmv_info * out)
 	out->stored_elems = h.stored_elems;
 	out->device_bytes = h.device_bytes;
 	out->convert_ms = h.convert_ms;
+	out->alloc_ms = h.alloc_ms;
+	out->copy_in_ms = h.copy_in_ms;
 	out->kernels_per_run = h.kernels_per_run;
 	out->format = h.desc.format;
 	snprintf(out->format_name, sizeof(out->format_name), "%s", h.name.c_str());

@@ -113,6 +113,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t * bar, uint32_t parit
 	return true;
 }
 
+// Before a CTA (or warp) that gave up on a wait leaves: waits, bounded, for the `pending`
+// bulk copies it issued that nobody has waited for, ring slots s, s+1, ... (mod S) from
+// phase `parity` on, so that no copy is still writing into the shared memory of a CTA
+// that has exited.  A slot whose copy already landed returns at once.
+__device__ __forceinline__ void drain_ring(uint64_t * bars, int S, int s, uint32_t parity, int pending,
+		long long budget)
+{
+	for (int q = 0; q < pending; q++) {
+		(void) mbar_wait_bounded(&bars[s], parity, budget);
+		if (++s == S) {
+			s = 0;
+			parity ^= 1u;
+		}
+	}
+}
+
 // Named barrier over n threads (a multiple of 32) of the CTA.
 __device__ __forceinline__ void named_bar_sync(int id, int n)
 {
@@ -171,5 +187,14 @@ __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b)
 static constexpr int WS_GATHER_SLOTS = SPMV_WS_GATHER_SLOTS;
 
 static constexpr long long kWaitBudgetCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+// Bound of a device wait in clock cycles for a limit given in microseconds (0: the default
+// ~2 s).  2,000 cycles a microsecond is at or above the B200's top SM clock (1,965 MHz), so
+// a wait lasts at least the stated time.
+__host__ __device__ __forceinline__ long long wait_budget_cycles(int limit_us)
+{
+	return limit_us > 0 ? (long long) limit_us * 2000LL : kWaitBudgetCycles;
+}
+
 
 }  // namespace spmv

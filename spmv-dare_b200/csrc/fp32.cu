@@ -11,6 +11,8 @@
 // block's contiguous (values, columns) range into shared memory, a CTA-wide x gather, then
 // one thread per row; a row longer than a block is reduced by the whole CTA with a
 // compensated tree.
+#include <atomic>
+
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -106,8 +108,13 @@ __global__ void __launch_bounds__(F32_THREADS) f32_kernel(F32Args a)
 		const StagedBlock d = a.blocks[b];
 		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
-			if (threadIdx.x == 0)
+			if (threadIdx.x == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				int pending = 0;          // copies issued for blocks b, b + grid, ... not yet waited for
+				while (pending < a.stages && b + (int64_t) pending * gridDim.x < a.nblocks)
+					pending++;
+				drain_ring(bars, a.stages, s, parity, pending, kWaitBudgetCycles);
+			}
 			return;
 		}
 		if (d.units >= 0) {
@@ -192,6 +199,8 @@ struct F32WsArgs {
 	int stage_bytes;
 	int row_threads;
 	int * err;
+	long long wait_budget;   // bound of the kernel's waits, clock cycles
+	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
 };
 
 __device__ __forceinline__ void f32ws_issue(const F32WsArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
@@ -235,7 +244,7 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 		// ---- gather warps: x of every staged entry, WS_GATHER_SLOTS loads in flight per thread
 		const int gt = threadIdx.x;
 		for (int64_t b = b_begin; b < b_end; b++) {
-			const bool ok = mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles);
+			const bool ok = mbar_wait_bounded(&full[s], parity, a.wait_budget);
 			if (!__all_sync(0xffffffffu, ok)) {            // the warp leaves together
 				if ((gt & 31) == 0)
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
@@ -264,7 +273,7 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 				}
 			}
 			__syncwarp();                                  // the warp's stores before its arrival
-			if ((gt & 31) == 0)
+			if ((gt & 31) == 0 && !a.hold)
 				mbar_arrive(&prod[s]);
 			if (++s == S) {
 				s = 0;
@@ -299,10 +308,13 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 			js = (int) ((int64_t) __ldg(a.rp + r) - e0);
 			je = (int) ((int64_t) __ldg(a.rp + r + 1) - e0);
 		}
-		const bool ok = mbar_wait_bounded(&prod[s], parity, kWaitBudgetCycles);
+		const bool ok = mbar_wait_bounded(&prod[s], parity, a.wait_budget);
 		if (named_bar_or(1, nr, !ok)) {      // all row threads leave together
-			if (rt == 0)
+			if (rt == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				// rt 0 issued the copies of blocks b .. b + S - 1: wait until they have landed
+				drain_ring(full, S, s, parity, (int) (b_end - b < S ? b_end - b : S), kWaitBudgetCycles);
+			}
 			return;
 		}
 		const uint8_t * st = smem + (size_t) s * a.stage_bytes;
@@ -541,8 +553,10 @@ __global__ void __launch_bounds__(SEG_THREADS) f32seg_kernel(SegArgs a)
 	{
 		const bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitBudgetCycles);
 		if (!__all_sync(FULL, ok)) {
-			if (lane == 0)
+			if (lane == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				drain_ring(bars, S, 0, 0u, (int) (ce - cb < S ? ce - cb : S), kWaitBudgetCycles);
+			}
 			return;
 		}
 		const int4 * sc = reinterpret_cast<const int4 *>(wsm + SEG_CHUNK * 4) + 2 * lane;
@@ -561,8 +575,12 @@ __global__ void __launch_bounds__(SEG_THREADS) f32seg_kernel(SegArgs a)
 			// request x of the next chunk before summing this one
 			const bool ok = mbar_wait_bounded(&bars[ns], nparity, kWaitBudgetCycles);
 			if (!__all_sync(FULL, ok)) {
-				if (lane == 0)
+				if (lane == 0) {
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+					// copies in flight: chunks ch + 1 .. ch + S - 1 (the next one with S == 1)
+					const int64_t span = S > 1 ? S - 1 : 1;
+					drain_ring(bars, S, ns, nparity, (int) (ce - ch - 1 < span ? ce - ch - 1 : span), kWaitBudgetCycles);
+				}
 				return;
 			}
 			const int4 * sc = reinterpret_cast<const int4 *>(wsm + (size_t) ns * SEG_STAGE_BYTES + SEG_CHUNK * 4) + 2 * lane;
@@ -845,6 +863,8 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 		w.stage_bytes = f32ws_stage_bytes(w.cap_al);
 		w.row_threads = h.row_threads;
 		w.err = h.d_err;
+		w.wait_budget = wait_budget_cycles(h.desc.wait_limit_us);
+		w.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
 		ws_f32_kernel<<<h.grid, h.threads, h.smem_bytes, s>>>(w);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
@@ -872,27 +892,29 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 static __device__ __align__(256) float g_mixed_scratch[SPMV_NOALLOC_MAX_ELEMS];
 
 // Device address of g_mixed_scratch per device, resolved once per device (with that
-// device current) by the first call on it.
-static float * g_mixed_scratch_addr[64];
+// device current) by the first call on it.  Host threads that race on the first call
+// resolve the same address and store it atomically.  The cache does not survive
+// cudaDeviceReset(): the module is then loaded again and the array may move.
+static std::atomic<float *> g_mixed_scratch_addr[64];
 
-static int mixed_scratch(float ** out)
+static int mixed_scratch(int dev, float ** out)
 {
-	int dev = 0;
-	SPMV_CUDA_TRY(cudaGetDevice(&dev));
 	if (dev < 0 || dev >= 64) {
 		set_error(SPMV_ERR_ARG, "no-alloc entry: device ordinal %d out of range", dev);
 		return SPMV_ERR_ARG;
 	}
-	if (!g_mixed_scratch_addr[dev]) {
+	float * p = g_mixed_scratch_addr[dev].load(std::memory_order_acquire);
+	if (!p) {
 		void * ptr = nullptr;
 		cudaError_t e = cudaGetSymbolAddress(&ptr, g_mixed_scratch);
 		if (e != cudaSuccess) {
 			set_error(SPMV_ERR_CUDA, "no-alloc entry: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
 			return SPMV_ERR_CUDA;
 		}
-		g_mixed_scratch_addr[dev] = static_cast<float *>(ptr);
+		p = static_cast<float *>(ptr);
+		g_mixed_scratch_addr[dev].store(p, std::memory_order_release);
 	}
-	*out = g_mixed_scratch_addr[dev];
+	*out = p;
 	return SPMV_OK;
 }
 
@@ -907,8 +929,15 @@ int run_mixed_noalloc(Handle & h, const double * d_x, double * d_y, cudaStream_t
 				(long long) (h.n + h.m), (int) SPMV_NOALLOC_MAX_ELEMS);
 		return SPMV_ERR_ARG;
 	}
+	int dev = -1;
+	SPMV_CUDA_TRY(cudaGetDevice(&dev));
+	if (dev != h.device) {
+		// the array is per device: another GPU's copy would be read through peer access or fault
+		set_error(SPMV_ERR_ARG, "no-alloc entry: the handle lives on device %d but device %d is current", h.device, dev);
+		return SPMV_ERR_ARG;
+	}
 	float * scratch = nullptr;
-	SPMV_TRY(mixed_scratch(&scratch));
+	SPMV_TRY(mixed_scratch(dev, &scratch));
 	float * xf = scratch;            // x rounded to FP32: written in full before it is read
 	float * yf = scratch + h.n;      // FP32 y: every row is written by the SpMV kernel
 	SPMV_TRY(convert_vector_d2f(d_x, xf, h.n, s));

@@ -1,6 +1,7 @@
 // Internal state of a converted matrix (the GPU counterpart of one Matrix_Format object).
 #pragma once
 
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -160,6 +161,8 @@ struct Handle {
 	int64_t stored_elems = 0;
 	int64_t device_bytes = 0;
 	double convert_ms = 0;
+	double alloc_ms = 0;        // host time inside cudaMalloc during the conversion
+	double copy_in_ms = 0;      // the CSR arrays' copy to the device (until it completed)
 	int kernels_per_run = 0;
 	std::string name;
 
@@ -167,7 +170,9 @@ struct Handle {
 	int alloc(T ** p, int64_t count)
 	{
 		size_t bytes = (size_t) (count > 0 ? count : 1) * sizeof(T);
+		const auto t0 = std::chrono::steady_clock::now();
 		cudaError_t e = cudaMalloc((void **) p, bytes);
+		alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 		if (e != cudaSuccess) {
 			*p = nullptr;
 			set_error(SPMV_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));

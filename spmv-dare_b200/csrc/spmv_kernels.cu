@@ -48,6 +48,8 @@ struct StagedArgs {
 	int cols_off;            // warp-specialised kernel: byte offset of the staged columns in a stage
 	const int64_t * ranges;  // warp-specialised kernel: each CTA's contiguous block range
 	int * err;
+	long long wait_budget;   // bound of the warp-specialised kernel's waits, clock cycles
+	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
 };
 
 // Sequential sum of s[0..n) in index order.
@@ -457,8 +459,13 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) staged_kernel(StagedArgs a
 			dnext = a.blocks[nb];
 		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
-			if (threadIdx.x == 0)
+			if (threadIdx.x == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				int pending = 0;          // copies issued for blocks b, b + grid, ... not yet waited for
+				while (pending < a.stages && b + (int64_t) pending * gridDim.x < a.nblocks)
+					pending++;
+				drain_ring(bars, a.stages, s, parity, pending, kWaitBudgetCycles);
+			}
 			return;
 		}
 		const StagedBlock d = sdesc[s];
@@ -555,8 +562,13 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) pipe_kernel(StagedArgs a)
 	{
 		const bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
-			if (threadIdx.x == 0)
+			if (threadIdx.x == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				int pending = 0;          // the first S blocks' copies
+				while (pending < S && b + (int64_t) pending * gridDim.x < a.nblocks)
+					pending++;
+				drain_ring(bars, S, 0, 0u, pending, kWaitBudgetCycles);
+			}
 			return;
 		}
 		if (d.units >= 0) {
@@ -580,8 +592,16 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) pipe_kernel(StagedArgs a)
 			dn = a.blocks[nb];
 			const bool ok = mbar_wait_bounded(&bars[ns], nparity, kWaitBudgetCycles);
 			if (__syncthreads_or(!ok)) {
-				if (threadIdx.x == 0)
+				if (threadIdx.x == 0) {
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+					// copies in flight: blocks nb, nb + grid, ... up to the last one issued,
+					// b + (S - 1) * grid (S - 1 of them; the one next block with S == 1)
+					const int span = S > 1 ? S - 1 : 1;
+					int pending = 0;
+					while (pending < span && nb + (int64_t) pending * gridDim.x < a.nblocks)
+						pending++;
+					drain_ring(bars, S, ns, nparity, pending, kWaitBudgetCycles);
+				}
 				return;
 			}
 			if (dn.units >= 0)
@@ -842,7 +862,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		// ---- gather warps
 		const int gt = threadIdx.x;
 		for (int64_t b = b_begin; b < b_end; b++) {
-			const bool ok = mbar_wait_bounded(&full[s], parity, kWaitBudgetCycles);
+			const bool ok = mbar_wait_bounded(&full[s], parity, a.wait_budget);
 			if (named_bar_or(2, ng, !ok)) {                // the gather warps leave together
 				if (gt == 0)
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
@@ -887,7 +907,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 				}
 			}
 			__syncwarp();                                  // the warp's stores before its arrival
-			if ((gt & 31) == 0)
+			if ((gt & 31) == 0 && !a.hold)
 				mbar_arrive(&prod[s]);
 			if (++s == S) {
 				s = 0;
@@ -922,10 +942,13 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		int js0 = 0, je0 = 0;
 		int64_t yi = -1;
 		row_pre_t<K, YMAP>(a, d, rt, js0, je0, yi);
-		const bool ok = mbar_wait_bounded(&prod[s], parity, kWaitBudgetCycles);
+		const bool ok = mbar_wait_bounded(&prod[s], parity, a.wait_budget);
 		if (named_bar_or(1, nr, !ok)) {      // all row threads leave together
-			if (rt == 0)
+			if (rt == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				// rt 0 issued the copies of blocks b .. b + S - 1: wait until they have landed
+				drain_ring(full, S, s, parity, (int) (b_end - b < S ? b_end - b : S), kWaitBudgetCycles);
+			}
 			return;
 		}
 		uint8_t * st = smem + (size_t) s * a.stage_bytes;
@@ -998,8 +1021,10 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) batch_kernel(BatchArgs b)
 	for (;; ) {
 		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (__syncthreads_or(!ok)) {
-			if (threadIdx.x == 0)
+			if (threadIdx.x == 0) {
 				dev_flag_error(b.err, DEV_ERR_TIMEOUT);
+				drain_ring(bars, b.stages, s, parity, b.stages, kWaitBudgetCycles);   // every slot holds a claim
+			}
 			return;
 		}
 		const int64_t c = claim[s];
@@ -1495,6 +1520,8 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.stage_bytes = (int) (ceil_div((int64_t) a.cap_al * 12, 128) * 128);
 	a.exact = h.desc.exact;
 	a.err = h.d_err;
+	a.wait_budget = wait_budget_cycles(h.desc.wait_limit_us);
+	a.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
 	if (fmt == SPMV_FMT_CSR_NAIVE || fmt == SPMV_FMT_CSR_VEC) {
 		a.ptr = h.d_rp;
 		a.cols = h.d_ci;

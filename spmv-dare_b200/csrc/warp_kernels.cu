@@ -115,8 +115,11 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) warp_kernel(WarpArgs a)
 		const WarpChunk d = a.chunks[c];
 		bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (!__all_sync(0xffffffffu, ok)) {
-			if (lane == 0)
+			if (lane == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				// lane 0 issued the copies of chunks c .. c + stages - 1
+				drain_ring(bars, a.stages, s, parity, (int) (ce - c < a.stages ? ce - c : a.stages), kWaitBudgetCycles);
+			}
 			return;
 		}
 		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
@@ -331,8 +334,11 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) tiled_warp_kernel(WarpArgs a
 		const WarpChunk d = a.chunks[c];
 		const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitBudgetCycles);
 		if (!__all_sync(0xffffffffu, ok)) {
-			if (lane == 0)
+			if (lane == 0) {
 				dev_flag_error(a.err, DEV_ERR_TIMEOUT);
+				// lane 0 issued the copies of chunks c .. c + stages - 1
+				drain_ring(bars, a.stages, s, parity, (int) (ce - c < a.stages ? ce - c : a.stages), kWaitBudgetCycles);
+			}
 			return;
 		}
 		// chunks start at slice starts or tile boundaries (multiples of 32 entries): off == 0

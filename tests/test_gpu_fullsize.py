@@ -2,8 +2,11 @@
 config 2: 4M rows, nnz 80,469,735), generated by the native generator (itself pinned on
 the reference generator) with values mapped v -> 2v - 1 and x ~ U[-1, 1).
 
-Against the oracle restatement (which is pinned on the reference): y bit-identical per
-format, converted arrays bit-identical; against binary128 row sums: within 1e-12.
+Against the reference compiled from its own sources (oracle/_ref, the reference's
+csr_to_format + Matrix_Format::spmv of each format, T = 8 threads): every converted array
+and every y bit-identical at both sizes.  SELL-C-sigma's RVV kernel cannot run on x86, so
+its y is compared with the oracle restatement (its arrays with the compiled reference
+conversion).  Against binary128 row sums: within 1e-12.
 """
 import numpy as np
 import pytest
@@ -93,6 +96,82 @@ def test_other_formats_config2_properties(sb, orc, fmt):
         a = mf.export("a")
         assert np.count_nonzero(a) == np.count_nonzero(v)
         assert np.isclose(np.sum(np.abs(a)), np.sum(np.abs(v)), rtol=1e-12)
+
+
+def _need_ref(orc, fmt):
+    if not orc.ref_available(fmt):
+        pytest.fail(f"the compiled reference for {fmt} is missing (make -C oracle ref)")
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted"])
+def test_against_compiled_reference(sb, orc, cfg, fmt):
+    """Converted arrays (row_cluster_ptr, ja, a, thread ranges, permutations) and y bit for
+    bit against the reference's own csr_to_format + spmv (csr.cpp, csr_vec.cpp,
+    sell.cpp:95-280, sell_sorted.cpp:119-427), y probed with the bench's m + 64 buffer of
+    ones (bench_spmv.cpp:561-564)."""
+    _need_ref(orc, fmt)
+    rp, ci, v, x = matrix(sb, cfg)
+    mf = sb.csr_to_format(rp, ci, v, format=fmt)
+    y = mf.spmv(x, np.full(mf.m, 1.0))
+    R = orc.RefFormat(fmt, rp, ci, v, threads=T)
+    try:
+        y_ref = R.spmv(x)[:mf.m]
+        if fmt in ("sell", "sell_sorted"):
+            for k, a in R.sell_arrays().items():
+                got = np.ascontiguousarray(mf.export(k))
+                assert got.dtype == a.dtype and np.array_equal(got.view(np.uint8), a.view(np.uint8)), k
+        assert mf.mem_footprint == R.mem_footprint
+    finally:
+        R.close()
+    bad = np.flatnonzero(_bits(y) != _bits(y_ref))
+    assert bad.size == 0, f"{bad.size} rows differ from the reference, first {bad[:5]}"
+
+
+@pytest.mark.parametrize("cfg,C,sigma", [("config1", 32, 256), ("config2", 32, 512)])
+def test_sellcs_arrays_against_compiled_reference(sb, orc, cfg, C, sigma):
+    """SELL-C-sigma conversion against the reference's own sellcs_format.c / radix_sort.c
+    (get_order_by_row_size, csr_to_sellcs), compiled from its sources."""
+    _need_ref(orc, "sellcs")
+    rp, ci, v, x = matrix(sb, cfg)
+    mf = sb.csr_to_format(rp, ci, v, format="sell_c_s", sellcs_c=C, sellcs_sigma=sigma)
+    ref = orc.ref_sellcs_convert(rp, ci, v, C, sigma)
+    names = {"row_order": "row_order", "slice_widths": "slice_widths", "slice_pointers": "slice_pointers",
+             "column_indices": "column_indices", "values": "sellcs_values"}
+    for k, a in ref.items():
+        got = mf.export(names[k])
+        if k == "values":
+            assert np.array_equal(_bits(got), _bits(a)), k
+        else:
+            assert np.array_equal(got.astype(np.int64), a.astype(np.int64)), k
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_div_rf_against_compiled_reference(sb, orc, cfg):
+    """DIV-RF packet bytes and packet-group offsets bit for bit against the reference's
+    own compress_kernel_div (div.cpp:236-604, div_kernels_rf.h:538-919) at T = 8, L = 4,
+    16384 values a packet; y within 1e-12 of the reference's decoder (its sums run in
+    value-sorted order, as do ours, but the partial sums of split rows combine
+    differently)."""
+    _need_ref(orc, "div_rf")
+    rp, ci, v, x = matrix(sb, cfg)
+    mf = sb.csr_to_format(rp, ci, v, format="div_rf")
+    data, groups = mf.export("div_data"), mf.export("div_groups")
+    y = mf.spmv(x, np.full(mf.m, 1.0))
+    R = orc.RefFormat("div_rf", rp, ci, v, threads=T)
+    try:
+        a = R.div_arrays()
+        y_ref = R.spmv(x)[:mf.m]
+    finally:
+        R.close()
+    assert np.array_equal(mf.export("div_thread_bytes"), a["thread_bytes"])
+    ref_data = orc.div_zero_header_padding(a["data"], V)
+    bad = np.flatnonzero(data != ref_data)
+    assert data.size == ref_data.size and bad.size == 0, f"{bad.size} packet bytes differ, first {bad[:5]}"
+    assert np.array_equal(groups, a["group_pos"])
+    gold, absy = orc.csr_gold(rp, ci, v, x)
+    assert rel_row_error(y, y_ref, absy) <= TOL
+    assert rel_row_error(y, gold, absy) <= TOL
 
 
 @pytest.mark.parametrize("cfg", ["config1", "config2"])
