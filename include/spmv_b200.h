@@ -328,6 +328,34 @@ int64_t spmv_artgen_nnz(const spmv_artgen * g);
 int spmv_artgen_get(const spmv_artgen * g, int32_t * row_ptr, int32_t * col_ind, double * values, double * stats);
 void spmv_artgen_destroy(spmv_artgen * g);
 
+/* ---------------------------------------------------------------- Matrix-Market import */
+/*
+ * The reference's real-matrix path (src/bench.cpp:127-238): mtx_read(filename,
+ * expand_symmetry, pattern values 1.0) + mtx_values_convert_to_real
+ * (lib/storage_formats/matrix_market/matrix_market.c:258-331, :421-463) + coo_to_csr with
+ * sorted columns (lib/storage_formats/csr/csr_gen.c:178-210).  The text is parsed on the
+ * host (strtol / strtod); COO -> CSR runs on the GPU.  expand_symmetry = 0 keeps a
+ * symmetric file's stored triangle (the reference's KEEP_SYMMETRY build); its CSR is then
+ * flagged symmetric and not expanded, which spmv_create() rejects as the reference's formats
+ * do (csr.cpp:131).  Coordinate files only (the reference's import has no path for the
+ * dense array format).  spmv_mtx_read returns NULL + *status on error (message in
+ * spmv_last_error()).
+ */
+typedef struct spmv_mtx spmv_mtx;
+spmv_mtx * spmv_mtx_read(const char * filename, int32_t expand_symmetry, int * status);
+int spmv_mtx_info(const spmv_mtx * mtx, int64_t * m, int64_t * n, int64_t * nnz, int32_t * symmetric,
+		int32_t * symmetry_expanded, int64_t * nnz_diag, int64_t * nnz_non_diag);
+/* Copies row_ptr int32[m+1], col_ind int32[nnz], values f64[nnz] (any may be NULL). */
+int spmv_mtx_get(const spmv_mtx * mtx, int32_t * row_ptr, int32_t * col_ind, double * values);
+void spmv_mtx_destroy(spmv_mtx * mtx);
+
+/* coo_to_csr(R, C, V, m, n, nnz, row_ptr, col_idx, values, sort_columns = 1, transpose = 0)
+ * (csr_gen.c:178-210) on device arrays, enqueued on `stream`; d_vals may be NULL (values
+ * 1.0).  Every row's entries come out sorted by column; entries repeated at one coordinate
+ * keep their input order.  SPMV_ERR_CSR if a coordinate lies outside m x n. */
+int spmv_coo_to_csr_device(const int32_t * d_rows, const int32_t * d_cols, const double * d_vals, int64_t m,
+		int64_t n, int64_t nnz, int32_t * d_row_ptr, int32_t * d_col_ind, double * d_values, void * stream);
+
 /* Library version string. */
 const char * spmv_version(void);
 

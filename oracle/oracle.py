@@ -302,6 +302,12 @@ def _ref(name):
             L.ref_gen_free.argtypes = [c_void_p]
             L.ref_cross_row_similarity.restype = c_double
             L.ref_cross_row_similarity.argtypes = [c_void_p, c_void_p, c_long, c_long, c_long, c_int]
+        elif name == "mtx":
+            L.ref_mtx_import.restype = c_void_p
+            L.ref_mtx_import.argtypes = [c_char_p, c_long, c_int]
+            L.ref_mtx_info.argtypes = [c_void_p, c_void_p]
+            L.ref_mtx_arrays.argtypes = [c_void_p] * 4
+            L.ref_mtx_free.argtypes = [c_void_p]
         elif name == "sellcs":
             L.ref_sellcs_convert.restype = c_void_p
             L.ref_sellcs_convert.argtypes = [c_void_p] * 3 + [c_long] * 5
@@ -425,6 +431,26 @@ class RefFormat:
         return dict(data=np.concatenate(streams) if streams else np.empty(0, np.uint8),
                     thread_bytes=np.array([s.size for s in streams], np.int64),
                     group_pos=np.concatenate(groups), ranges=ranges, T=T)
+
+
+def ref_read_mtx(path, expand_symmetry=True, threads=4):
+    """The reference's import_file (src/bench.cpp:127-238) on a well-formed Matrix-Market
+    file: dict of CSR arrays and the m, n, nnz, nnz_diag, nnz_non_diag, symmetric and
+    expanded flags."""
+    L = _ref("mtx")
+    h = L.ref_mtx_import(os.fsencode(path), 1 if expand_symmetry else 0, threads)
+    try:
+        info = np.zeros(7, np.int64)
+        L.ref_mtx_info(h, _p(info))
+        m, n, nnz = int(info[0]), int(info[1]), int(info[2])
+        rp = np.zeros(m + 1, np.int32)
+        ci = np.zeros(max(nnz, 1), np.int32)
+        v = np.zeros(max(nnz, 1), np.float64)
+        L.ref_mtx_arrays(h, _p(rp), _p(ci), _p(v))
+    finally:
+        L.ref_mtx_free(h)
+    return dict(row_ptr=rp, col_ind=ci[:nnz], values=v[:nnz], m=m, n=n, nnz=nnz, nnz_diag=int(info[3]),
+                nnz_non_diag=int(info[4]), symmetric=int(info[5]), expanded=int(info[6]))
 
 
 def ref_sellcs_convert(rp, ci, v, C, sigma):

@@ -29,7 +29,8 @@ from ._capi import FORMATS, VALUES_F32, VALUES_F64
 
 __all__ = [
     "SpmvError", "Matrix_Format", "csr_to_format", "statistics_print_labels", "generate_artificial",
-    "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version", "Batch",
+    "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version", "Batch", "read_mtx", "MtxMatrix",
+    "coo_to_csr",
 ]
 
 
@@ -406,3 +407,67 @@ def generate_artificial(rows, cols, avg_nnz_per_row, std_nnz_per_row, distributi
                   distribution=distribution, placement=placement, avg_bw=avg_bw, skew=skew,
                   avg_num_neighbours=avg_num_neighbours, cross_row_similarity=cross_row_similarity, seed=seed)
     return ArtificialMatrix(rp, ci[:nnz], v[:nnz], dict(zip(STAT_NAMES, stats.tolist())), params)
+
+
+class MtxMatrix:
+    """CSR arrays of an imported Matrix-Market file, with the reference's CSR_reference_s
+    flags (src/bench.cpp:196-207): symmetric, symmetry_expanded, nnz_diag, nnz_non_diag."""
+
+    def __init__(self, row_ptr, col_ind, values, n, symmetric, symmetry_expanded, nnz_diag, nnz_non_diag):
+        self.row_ptr, self.col_ind, self.values = row_ptr, col_ind, values
+        self.n = n
+        self.symmetric, self.symmetry_expanded = symmetric, symmetry_expanded
+        self.nnz_diag, self.nnz_non_diag = nnz_diag, nnz_non_diag
+
+    @property
+    def m(self):
+        return self.row_ptr.size - 1
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+
+def read_mtx(path, expand_symmetry=True):
+    """The reference's import_file (src/bench.cpp:127-238) for a Matrix-Market coordinate
+    file: parsed on the host, COO -> CSR (columns sorted in every row) on the GPU.
+    expand_symmetry=False keeps a symmetric file's stored triangle (KEEP_SYMMETRY)."""
+    import os
+
+    lib = library()
+    st = c_int(0)
+    x = lib.spmv_mtx_read(os.fsencode(path), 1 if expand_symmetry else 0, byref(st))
+    if not x:
+        _raise(st.value)
+    try:
+        m, n, nnz, nd, nn = c_int64(), c_int64(), c_int64(), c_int64(), c_int64()
+        sym, exp = ctypes.c_int32(), ctypes.c_int32()
+        lib.spmv_mtx_info(x, byref(m), byref(n), byref(nnz), byref(sym), byref(exp), byref(nd), byref(nn))
+        rp = np.empty(m.value + 1, np.int32)
+        ci = np.empty(max(nnz.value, 1), np.int32)
+        v = np.empty(max(nnz.value, 1), np.float64)
+        lib.spmv_mtx_get(x, rp.ctypes.data, ci.ctypes.data, v.ctypes.data)
+    finally:
+        lib.spmv_mtx_destroy(x)
+    return MtxMatrix(rp, ci[:nnz.value], v[:nnz.value], n.value, sym.value, exp.value, nd.value, nn.value)
+
+
+def coo_to_csr(rows, cols, values, m, n):
+    """coo_to_csr (csr_gen.c:178-210, sorted columns) on the GPU for CUDA torch tensors
+    (int32 rows / cols, float64 values or None): returns (row_ptr, col_ind, values) tensors."""
+    import torch
+
+    nnz = int(rows.numel())
+    dev = rows.device
+    rp = torch.empty(int(m) + 1, dtype=torch.int32, device=dev)
+    ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    vv = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+    rows, cols = rows.contiguous(), cols.contiguous()
+    values = values.contiguous() if values is not None else None
+    st = library().spmv_coo_to_csr_device(rows.data_ptr(), cols.data_ptr(),
+                                          values.data_ptr() if values is not None else None,
+                                          int(m), int(n), nnz, rp.data_ptr(), ci.data_ptr(), vv.data_ptr(),
+                                          _torch_stream(dev))
+    if st:
+        _raise(st)
+    return rp, ci[:nnz], vv[:nnz]

@@ -109,6 +109,12 @@ SIGNATURES = {
     "spmv_batch_sync": (c_int, [c_void_p]),
     "spmv_batch_info": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_batch_destroy": (None, [c_void_p]),
+    "spmv_mtx_read": (c_void_p, [c_char_p, c_int32, POINTER(c_int)]),
+    "spmv_mtx_info": (c_int, [c_void_p] + [c_void_p] * 7),
+    "spmv_mtx_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_mtx_destroy": (None, [c_void_p]),
+    "spmv_coo_to_csr_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
 }
 
 _lib = None

@@ -488,8 +488,10 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		k = 2;                      // CSR: the warp kernel's own path
 	if (k == 8 && V < 8)
 		k = 4;                      // narrower slices already give a warp 8 neighbouring columns
-	if (k == 9 && V != 32)
-		k = V >= 8 ? 8 : 4;         // kernel 9's lane transpose takes slices of exactly 32 rows
+	if ((k == 9 || k == 10) && V != 32)
+		k = V >= 8 ? 8 : 4;         // kernels 9 and 10's lane transpose takes slices of exactly 32 rows
+	if (k == 10 && V == 1)
+		k = 4;
 	h.exec_kernel = k;
 	if (k == 1)
 		return SPMV_OK;
@@ -498,6 +500,10 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 	if (k == 9) {
 		SPMV_TRY(build_tiled_cols(h, d_P, U, V));
 		return build_warp_chunks(h, d_P, U, V);
+	}
+	if (k == 10) {
+		SPMV_TRY(build_tiled_cols(h, d_P, U, V));
+		return build_tile_reg(h, d_P, U, V);
 	}
 	staged_defaults(h);
 	if (k == 3 && h.desc.stages == 0)

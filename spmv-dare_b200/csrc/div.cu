@@ -787,6 +787,136 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 	}
 }
 
+// ------------------------------------------------------------------ warp decoder (32 lanes)
+// With L = 32 every lane stream of a packet belongs to one lane of a warp, and the lane walks
+// it once, in order: no scans over threads, every entry decoded once.  One warp per packet;
+// per position the code byte (the 32 lanes read 32 neighbouring bytes), the lane's payload
+// bytes through a streaming reader (two words in registers, one aligned 8-byte load per 8
+// bytes consumed), the coordinates (neighbouring for rf = 1) and x; products go to the
+// warp's row sums in shared memory, then the packet's rows are stored as in the CTA decoder.
+constexpr int DIVW_WARPS = 8;
+
+struct LaneReader {
+	const uint64_t * w;      // next aligned word to load
+	uint64_t cur, nxt;       // the words holding the read position and the one after it
+	int sh;                  // read position within cur, in bytes
+	__device__ __forceinline__ void init(const uint8_t * p)
+	{
+		const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+		w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t) 7);
+		sh = (int) (a & 7);
+		cur = w[0];
+		nxt = w[1];
+		w += 2;
+	}
+	// n <= 8 little-endian bytes; reads reach at most 15 bytes past the read position
+	__device__ __forceinline__ uint64_t read(int n)
+	{
+		const uint64_t v = sh ? ((cur >> (8 * sh)) | (nxt << (64 - 8 * sh))) : cur;
+		sh += n;
+		if (sh >= 8) {
+			sh -= 8;
+			cur = nxt;
+			nxt = *w++;
+		}
+		return n >= 8 ? v : (v & ((1ULL << (8 * n)) - 1));
+	}
+};
+
+__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
+{
+	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	const int64_t p = (int64_t) blockIdx.x * DIVW_WARPS + wib;
+	if (p >= a.npackets)
+		return;
+	double * ys = ys_all[wib];
+	const uint8_t * h = a.data + a.pkt_off[p];
+	const int64_t nrows = ld_u32(h + 8);
+	const int64_t row_min = ld_u32(h + 12), col_min = ld_u32(h + 16);
+	const int row_bits = h[20], col_bits = h[21];
+	const int nrf = (int) ld_u32(h + 24);
+	const int cb = (row_bits + col_bits + 7) >> 3;
+	const int64_t nv = ld_u32(h + 0), nu = ld_u32(h + 4);
+	const uint8_t * rfs = h + 28 + 4 * 32;
+	const uint8_t * nus = rfs + 4 * nrf;
+	const uint8_t * coords = nus + 4 * nrf;
+	const uint8_t * codes = coords + cb * nv;
+	const uint8_t * lanes = codes + nu;
+	const uint64_t rmask = row_bits ? ((1ULL << row_bits) - 1) : 0;
+	const uint64_t cmask = (col_bits >= 64) ? ~0ULL : ((1ULL << col_bits) - 1);
+	for (int r = lane; r < nrows && r < DEC_MAX_ROWS; r += 32)
+		ys[r] = 0.0;
+	// lane i's stream starts after the streams of lanes < i
+	const uint32_t my_bytes = ld_u32(h + 28 + 4 * lane);
+	uint32_t start = my_bytes;
+	#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const uint32_t o = __shfl_up_sync(0xffffffffu, start, d);
+		if (lane >= d)
+			start += o;
+	}
+	start -= my_bytes;
+	LaneReader rd;
+	rd.init(lanes + start);
+	__syncwarp();
+	int kstart = 0, cstart = 0;
+	for (int g = 0; g < nrf; g++) {
+		const int rf = (int) ld_u32(rfs + 4 * g), u = (int) ld_u32(nus + 4 * g);
+		const int dv = u >> 5, md = u & 31;
+		const int n_i = dv + (lane < md ? 1 : 0);
+		uint64_t val = 0;                                   // differences restart in every group
+		if (rf == 1) {
+			for (int pos0 = 0; pos0 < n_i; pos0 += 4) {
+				double vv[4], xv[4];
+				int rr[4];
+				#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					const int pos = pos0 + q;
+					if (pos < n_i) {
+						const int k = pos * 32 + lane;
+						const uint8_t code = codes[kstart + k];
+						val += rd.read(code & 15) << ((code >> 4) << 2);
+						vv[q] = __longlong_as_double((long long) val);
+						const uint64_t c = ld_bytes(coords + (int64_t) (cstart + k) * cb, cb);
+						rr[q] = (int) (c & rmask);
+						xv[q] = __ldg(a.x + col_min + (int64_t) ((c >> row_bits) & cmask));
+					}
+				}
+				#pragma unroll
+				for (int q = 0; q < 4; q++)
+					if (pos0 + q < n_i)
+						atomicAdd(&ys[rr[q]], vv[q] * xv[q]);
+			}
+		} else {
+			for (int pos = 0; pos < n_i; pos++) {
+				const uint8_t code = codes[kstart + pos * 32 + lane];
+				val += rd.read(code & 15) << ((code >> 4) << 2);
+				const double vd = __longlong_as_double((long long) val);
+				for (int j = 0; j < rf; j++) {
+					const int k = (pos < dv) ? (pos * 32) * rf + 32 * j + lane : (dv * 32 + lane) * rf + j;
+					const uint64_t c = ld_bytes(coords + (int64_t) (cstart + k) * cb, cb);
+					atomicAdd(&ys[(int) (c & rmask)], vd * __ldg(a.x + col_min + (int64_t) ((c >> row_bits) & cmask)));
+				}
+			}
+		}
+		kstart += u;
+		cstart += rf * u;
+	}
+	__syncwarp();
+	const int4 mt = a.meta[p];
+	for (int64_t r = (int64_t) mt.x + lane; r < (int64_t) mt.y; r += 32) {
+		const int64_t rel = r - row_min;
+		if (rel < 0 || rel >= nrows) {
+			a.y[r] = 0.0;                                // empty rows between packets
+		} else if ((rel == 0 && (mt.z & 1)) || (rel == nrows - 1 && (mt.z & 2))) {
+			atomicAdd(&a.y[r], ys[rel]);                 // a row split across packets
+		} else {
+			a.y[r] = ys[rel];
+		}
+	}
+}
+
 __global__ void zero_rows_kernel(const int32_t * rows, int64_t n, double * y)
 {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -815,6 +945,13 @@ int convert_div(Handle & h)
 	const int64_t m = h.m, nnz = h.nnz;
 	if (L > DEC_THREADS) {
 		set_error(SPMV_ERR_ARG, "DIV-RF: vec_len %d above %d", L, DEC_THREADS);
+		return SPMV_ERR_ARG;
+	}
+	// decoder: 2 = one warp per packet, one lane per lane stream (32 lanes only; the default
+	// there); 0 = one CTA per packet, lanes shared by several threads (any lane count)
+	h.exec_kernel = h.desc.kernel < 0 ? (L == 32 ? 2 : 0) : h.desc.kernel;
+	if (h.exec_kernel != 0 && !(h.exec_kernel == 2 && L == 32)) {
+		set_error(SPMV_ERR_ARG, "DIV-RF: kernel %d unavailable (0, or 2 with vec_len 32)", h.desc.kernel);
 		return SPMV_ERR_ARG;
 	}
 	// dropped mantissa bits of the lossy mode (reduce_precision, div_kernels_rf.h:467-510)
@@ -1100,7 +1237,10 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.L = h.desc.vec_len;
 	a.x = d_x;
 	a.y = d_y;
-	div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
+	if (h.exec_kernel == 2)
+		div_warp_kernel<<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
+	else
+		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;
 }

@@ -104,7 +104,10 @@ struct Handle {
 	                             // own-gather, 6 warp-autonomous own-gather, 7 FP32 segmented,
 	                             // 8 warp-specialised over tiled slice columns
 	int row_threads = 0;         // kernels 4 and 8: threads of the row warps (the rest gather)
-	int32_t * d_tcols = nullptr; // kernel 8: slice column indices, row-major in 8-column tiles
+	int32_t * d_tcols = nullptr; // kernels 8-10: slice column indices, row-major in 8-column tiles
+	int2 * d_items = nullptr;    // kernel 10: work items (slice ranges), heaviest first
+	int64_t num_items = 0;
+	unsigned int * d_queue = nullptr;  // kernel 10: work-queue head and finished-warp count
 
 	// warp-autonomous kernel
 	WarpChunk * d_chunks = nullptr;
@@ -201,6 +204,7 @@ int convert_vector_f2d(const float * in, double * out, int64_t n, cudaStream_t s
 // with V = 1, or a slice pointer with slice height V).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V);
 int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V);
+int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V);
 int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
 
 // ---- SpMV launches

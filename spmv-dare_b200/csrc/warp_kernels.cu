@@ -12,6 +12,9 @@
 //   4. lane 0 refills the stage with the chunk `stages` ahead.
 // A row / slice larger than one chunk spans consecutive chunks of the same warp and its
 // accumulators live in registers across them (flags CONT_PREV / CONT_NEXT).
+#include <algorithm>
+#include <vector>
+
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -402,6 +405,115 @@ __global__ void __launch_bounds__(WARP_CTA_THREADS) tiled_warp_kernel(WarpArgs a
 	}
 }
 
+// ------------------------------------------------------------------ register-tiled slice kernel (kernel 10)
+// 32-row slices (SELL-C-sigma with C = 32, or SELL with V = 32) over the same tiled column
+// indices, without shared memory: a warp claims work items (runs of slices, the heaviest
+// ones first) from a queue and sums each slice's 32 rows straight from global memory.  Per
+// tile of 8 slice columns, lane L loads 8 tiled column indices (tile entry q * 32 + L: four
+// 128-byte requests' worth of one contiguous 1 KB) and the 8 values of its row
+// R = 4 (L % 8) + L / 8 (column-major: for each column the 32 lanes read one 256-byte
+// segment), both with streaming loads (evict first, so x keeps its place in L2); the
+// next tile's indices and values are requested before this tile's x, so DRAM latency
+// overlaps the x gather and the FMA chain.  x is transposed between lanes as in kernel 9
+// and each lane runs its row's FMA chain in column order, padding included: y is the
+// reference's bit for bit.  No shared memory, so occupancy is set by registers alone.
+struct TileRegArgs {
+	const int2 * items;            // work items: slice ranges [x, y)
+	int64_t nitems;
+	const int32_t * sptr;          // slice pointers (32-bit)
+	const int32_t * tcols;         // column indices, row-major in tiles of 8 slice columns
+	const double * vals;           // values, column-major per slice
+	const int32_t * ymap;          // row map (row_order / rev_permutation) or null
+	const double * x;
+	double * y;
+	int64_t m;
+	unsigned int * queue;          // [0] next item, [1] warps done: zero at launch, reset on exit
+	unsigned int total_warps;
+};
+
+constexpr int TILE_REG_THREADS = 256;
+
+__device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int lane, int R, int32_t (&c)[8],
+		double (&v)[8])
+{
+	#pragma unroll
+	for (int q = 0; q < 8; q++)
+		c[q] = __ldcs(a.tcols + t0 + q * 32 + lane);
+	#pragma unroll
+	for (int j = 0; j < 8; j++)
+		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
+}
+
+__device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int lane, int R)
+{
+	const int64_t b = a.sptr[sl];
+	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
+	const int nt = W >> 3, rem = W & 7;
+	double acc = 0.0;
+	int32_t c[8], cn[8];
+	double v[8], vn[8];
+	if (nt > 0)
+		tile_load(a, b, lane, R, c, v);
+	for (int t = 0; t < nt; t++) {
+		if (t + 1 < nt)
+			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, cn, vn);
+		double X[8];
+		#pragma unroll
+		for (int q = 0; q < 8; q++)
+			X[q] = __ldg(a.x + c[q]);
+		transpose8(X, lane);
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			acc = __fma_rn(v[j], X[j], acc);
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			c[j] = cn[j];
+			v[j] = vn[j];
+		}
+	}
+	if (rem > 0) {                               // the narrower last tile: rows at R * rem
+		const int64_t t0 = b + (int64_t) nt * 256;
+		double X[8], vv[8];
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			if (j < rem) {
+				X[j] = __ldg(a.x + __ldcs(a.tcols + t0 + R * rem + j));
+				vv[j] = __ldcs(a.vals + t0 + j * 32 + R);
+			}
+		}
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			if (j < rem)
+				acc = __fma_rn(vv[j], X[j], acc);
+	}
+	const int64_t row = sl * 32 + R;
+	if (row < a.m)
+		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
+}
+
+__global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
+{
+	const int lane = threadIdx.x & 31;
+	const int R = 4 * (lane & 7) + (lane >> 3);
+	for (;;) {
+		unsigned int it = 0;
+		if (lane == 0)
+			it = atomicAdd(&a.queue[0], 1u);
+		it = __shfl_sync(0xffffffffu, it, 0);
+		if ((int64_t) it >= a.nitems)
+			break;
+		const int2 r = a.items[it];
+		for (int64_t sl = r.x; sl < r.y; sl++)
+			tile_reg_slice(a, sl, lane, R);
+	}
+	// every warp has made its last claim before it counts itself done: the last one to
+	// finish puts the queue back to zero for the next launch
+	if (lane == 0 && atomicAdd(&a.queue[1], 1u) == a.total_warps - 1) {
+		atomicExch(&a.queue[0], 0u);
+		atomicExch(&a.queue[1], 0u);
+	}
+}
+
 using WarpFn = void (*)(WarpArgs);
 
 WarpFn pick_warp(const Handle & h)
@@ -638,8 +750,85 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 	return SPMV_OK;
 }
 
+// Work items of kernel 10: slices of at least TILE_REG_HEAVY entries alone, the heaviest
+// first; the others in matrix order, in runs of consecutive slices of about
+// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2).
+constexpr int64_t TILE_REG_HEAVY = 4096, TILE_REG_ITEM = 2048;
+
+int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
+{
+	if (V != 32) {
+		set_error(SPMV_ERR_ARG, "kernel 10 takes slices of exactly 32 rows (got %d)", V);
+		return SPMV_ERR_ARG;
+	}
+	cudaStream_t s = h.stream;
+	std::vector<int32_t> P((size_t) U + 1);
+	SPMV_CUDA_TRY(cudaMemcpyAsync(P.data(), d_P, (U + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	std::vector<int2> heavy, rest;
+	int64_t u = 0;
+	while (u < U) {
+		const int64_t len = (int64_t) P[u + 1] - P[u];
+		if (len >= TILE_REG_HEAVY) {
+			heavy.push_back(make_int2((int) u, (int) (u + 1)));
+			u++;
+			continue;
+		}
+		const int64_t u0 = u, e0 = P[u];
+		while (u < U && (int64_t) P[u + 1] - P[u] < TILE_REG_HEAVY && (int64_t) P[u] - e0 < TILE_REG_ITEM)
+			u++;
+		rest.push_back(make_int2((int) u0, (int) u));
+	}
+	std::stable_sort(heavy.begin(), heavy.end(), [&](const int2 & p, const int2 & q) {
+		return P[p.x + 1] - P[p.x] > P[q.x + 1] - P[q.x];
+	});
+	heavy.insert(heavy.end(), rest.begin(), rest.end());
+	h.num_items = (int64_t) heavy.size();
+	SPMV_TRY(h.alloc(&h.d_items, h.num_items));
+	if (h.num_items > 0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_items, heavy.data(), h.num_items * sizeof(int2), cudaMemcpyHostToDevice, s));
+	SPMV_TRY(h.alloc(&h.d_queue, 2));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
+	int per_sm = h.desc.ctas_per_sm;
+	if (per_sm <= 0) {
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel, TILE_REG_THREADS, 0));
+		if (per_sm < 1)
+			per_sm = 1;
+	}
+	h.grid = h.num_sms * per_sm;
+	h.threads = TILE_REG_THREADS;
+	h.smem_bytes = 0;
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	return SPMV_OK;
+}
+
 int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 {
+	if (h.exec_kernel == 10) {
+		if (h.num_items == 0)
+			return SPMV_OK;
+		TileRegArgs a{};
+		a.items = h.d_items;
+		a.nitems = h.num_items;
+		a.tcols = h.d_tcols;
+		a.x = d_x;
+		a.y = d_y;
+		a.m = h.m;
+		a.queue = h.d_queue;
+		a.total_warps = (unsigned int) h.grid * (TILE_REG_THREADS / 32);
+		if (h.desc.format == SPMV_FMT_SELL_C_S) {
+			a.sptr = h.d_sptr32;
+			a.vals = h.d_svals;
+			a.ymap = h.d_order;
+		} else {
+			a.sptr = h.d_rcp;
+			a.vals = h.d_a;
+			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
+		}
+		tile_reg_kernel<<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		SPMV_CUDA_TRY(cudaGetLastError());
+		return SPMV_OK;
+	}
 	if (h.num_chunks == 0)
 		return SPMV_OK;
 	const int fmt = h.desc.format;

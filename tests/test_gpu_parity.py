@@ -242,6 +242,32 @@ def test_tiled_kernel_long_slices(sb, orc):
                 assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
+@pytest.mark.parametrize("fmt,C,sigma", [("sell_c_s", 32, 512), ("sell_c_s", 32, 32), ("sell_c_s", 32, 4096),
+                                         ("sell", 32, 0), ("sell_sorted", 32, 0), ("sell_c_s", 64, 512)])
+def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma):
+    """Kernel 10 (warp-claimed slices of 32 rows summed from registers, no shared memory):
+    the reference's y bits on every golden case and on a skewed matrix whose heavy slices
+    (rows up to 3,000 entries) are claimed first; slice heights other than 32 fall back to
+    kernel 8.  Several launches in a row reuse the work queue, which each launch resets."""
+    kw = dict(sellcs_c=C, sellcs_sigma=sigma) if fmt == "sell_c_s" else dict(vec_len=C, num_threads=T)
+    cases = [load_golden(name) for name in golden_names()]
+    rng = np.random.default_rng(10)
+    m = n = 30000
+    lens = rng.integers(0, 40, m)
+    lens[rng.choice(m, 80, replace=False)] = rng.integers(200, 3000, 80)
+    lens[rng.choice(m, 700, replace=False)] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens]).astype(np.int32)
+    cases.append(dict(row_ptr=rp, col_ind=ci, values=rng.uniform(-1, 1, int(rp[-1])), x=rng.uniform(-1, 1, n), n=n))
+    for g in cases:
+        ref = (orc.sellcs_spmv(orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], C, sigma),
+                               g["row_ptr"].size - 1, C, g["x"]) if fmt == "sell_c_s" else _sliced_ref(orc, g, fmt, C))
+        mf = _mk(sb, g, fmt, kernel=10, **kw)
+        for _ in range(3):
+            y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+            assert _eq_bits(y, ref).size == 0, (fmt, C, sigma, g["row_ptr"].size - 1)
+
+
 def test_tiled_kernel_rejects_small_blocks(sb):
     g = load_golden("hand6")
     with pytest.raises(sb.SpmvError):           # a block must hold one 8 x 32 tile
@@ -391,6 +417,27 @@ def test_div_rf_other_lane_counts(sb, orc, name, L, pv, threads):
     y = mf.spmv(x, np.full(mf.m, 1.0))
     gold, absy = orc.csr_gold(rp, ci, v, x)
     assert rel_row_error(y, gold, absy) <= TOL
+
+
+@pytest.mark.parametrize("pv,threads", [(16384, 8), (4096, 8), (1000, 3), (64, 1)])
+def test_div_rf_warp_decoder(sb, orc, pv, threads):
+    """The 32-lane warp decoder (kernel 2: one warp per packet, one lane per lane stream)
+    against the CTA decoder (kernel 0) on the same packets and against binary128 row sums,
+    on every golden case (repeated values: rf > 1 groups; empty rows; long rows split over
+    packets) and twice in a row (split rows are zeroed before each run)."""
+    for name in golden_names():
+        g = load_golden(name)
+        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+        gold, absy = orc.csr_gold(rp, ci, v, x)
+        ys = {}
+        for kernel in (0, 2):
+            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel)
+            for _ in range(2):
+                ys[kernel] = mf.spmv(x, np.full(mf.m, 1.0))
+            assert rel_row_error(ys[kernel], gold, absy) <= TOL, (name, pv, kernel)
+        assert rel_row_error(ys[2], ys[0], absy) <= TOL
+    with pytest.raises(sb.SpmvError):
+        _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
 
 
 @pytest.mark.parametrize("tol", [1e-6, 1e-3])
