@@ -70,6 +70,9 @@ extern "C" {
  *                        (the reference hard-codes C=256, s=16384 at sell_c_s.cpp:58-60)
  *   div_packet_vals      CSRCV_NUM_PACKET_VALS (config.sh:150).                  default 16384
  *   div_tolerance        DIV_VC_TOLERANCE, lossy value rounding (config.sh:123). default 0
+ *   div_packet_reordering DIV_PACKET_REORDERING (config.sh:133): each thread's packet
+ *                        groups stored in ascending order of a median column
+ *                        (div.cpp:377-395, :455-498).                            default 0
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,
@@ -128,7 +131,8 @@ typedef struct spmv_format_desc {
 	int32_t threads;
 	int32_t wait_limit_us;
 	int32_t debug_flags;
-	int32_t reserved[4];
+	int32_t div_packet_reordering;
+	int32_t reserved[3];
 } spmv_format_desc;
 
 #define SPMV_DEBUG_WITHHOLD_HANDOFF 1

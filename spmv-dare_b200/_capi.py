@@ -53,7 +53,8 @@ class FormatDesc(ctypes.Structure):
         ("sellcs_sigma", c_int32), ("div_packet_vals", c_int32), ("div_tolerance", c_double),
         ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
         ("stages", c_int32), ("ctas_per_sm", c_int32), ("kernel", c_int32), ("threads", c_int32),
-        ("wait_limit_us", c_int32), ("debug_flags", c_int32), ("reserved", c_int32 * 4),
+        ("wait_limit_us", c_int32), ("debug_flags", c_int32), ("div_packet_reordering", c_int32),
+        ("reserved", c_int32 * 3),
     ]
 
 

@@ -81,6 +81,10 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "wait_limit_us must be in [0, 60e6] (got %d)", d.wait_limit_us);
 		return SPMV_ERR_ARG;
 	}
+	if (d.div_packet_reordering != 0 && d.div_packet_reordering != 1) {
+		set_error(SPMV_ERR_ARG, "div_packet_reordering must be 0 or 1 (got %d)", d.div_packet_reordering);
+		return SPMV_ERR_ARG;
+	}
 	if (d.debug_flags & ~SPMV_DEBUG_WITHHOLD_HANDOFF) {
 		set_error(SPMV_ERR_ARG, "unknown debug_flags bits 0x%x", d.debug_flags);
 		return SPMV_ERR_ARG;

@@ -30,6 +30,9 @@
 // shared memory.  The summation order inside a row differs from the reference's
 // value-sorted serial order, so DIV-RF y agrees with the reference within the stated
 // tolerance, not bit for bit.
+#include <algorithm>
+#include <vector>
+
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -917,11 +920,130 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 	}
 }
 
+// ------------------------------------------------------------------ packet reordering
+// DIV_PACKET_REORDERING (div.cpp:377-395, :455-498): every thread's packet groups are
+// stored in ascending order of a median column.  The reference records, per packet, the
+// median of its column indices (array_quantile_serial(ja, nv, 0.5), lib/array_metrics.c:
+// 952-1088, method "median_unbiased": with N values, N <= 2 gives the largest, even N the
+// order statistic N/2, odd N the mean of order statistics (N-1)/2 and (N+1)/2; truncated to
+// an integer) and then sorts the thread's groups g by the median of its g-th PACKET with its
+// quicksort.  Medians come from a GPU sort of (packet, column); the group permutation is
+// computed on the host with the reference's quicksort restated (ref_quicksort below: equal
+// keys end up where its partitioning puts them, so the same bytes result); the group byte
+// ranges are then moved on the GPU.
+__global__ void pkt_col_keys_kernel(const int32_t * pkt_of, const int32_t * ci, int64_t nnz, uint64_t * keys,
+		uint32_t * vals)
+{
+	const int64_t j = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= nnz)
+		return;
+	keys[j] = ((uint64_t) (uint32_t) pkt_of[j] << 32) | (uint64_t) (uint32_t) ci[j];
+	vals[j] = 0;
+}
+
+__global__ void pkt_median_kernel(const uint64_t * sorted, const int32_t * pk_j, const int32_t * pk_nv, int64_t NP,
+		int64_t * med)
+{
+	const int64_t p = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= NP)
+		return;
+	const int64_t b = pk_j[p], N = pk_nv[p];
+	const uint64_t * c = sorted + b;
+	if (N <= 2) {
+		med[p] = N > 0 ? (int64_t) (uint32_t) c[N - 1] : 0;
+	} else if ((N & 1) == 0) {
+		med[p] = (int64_t) (uint32_t) c[N / 2];
+	} else {
+		const double l = (double) (uint32_t) c[(N - 1) / 2], r = (double) (uint32_t) c[(N + 1) / 2];
+		med[p] = (int64_t) (__dadd_rn(__dmul_rn(0.5, l), __dmul_rn(0.5, r)));
+	}
+}
+
+__global__ void move_groups_kernel(const uint8_t * src, uint8_t * dst, const int64_t * plan, int64_t ngroups)
+{
+	// plan[3 g .. 3 g + 2]: source offset, destination offset, length of group g
+	const int64_t g = blockIdx.x;
+	if (g >= ngroups)
+		return;
+	const int64_t so = plan[3 * g], d = plan[3 * g + 1], len = plan[3 * g + 2];
+	for (int64_t i = threadIdx.x; i < len; i += blockDim.x)
+		dst[d + i] = src[so + i];
+}
+
 __global__ void zero_rows_kernel(const int32_t * rows, int64_t n, double * y)
 {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 		y[rows[i]] = 0.0;
+}
+
+// The reference's quicksort of an index array A[0..N) by key[A[i]] ascending
+// (lib/sort/quicksort/quicksort_gen.c:96-146 with partition_auto_serial /
+// partition_serial_base, lib/sort/partition/partition_gen.c:100-195), restated: a
+// median-of-three pivot, a two-cursor partition that swaps elements equal to the pivot, and
+// the reference's loop that keeps the left bounds on a stack and shrinks the right end by
+// one element per pop.  Equal keys end up where that procedure puts them.
+static int ref_cmp(int a, int b, const int * key)
+{
+	return key[a] > key[b] ? 1 : key[a] < key[b] ? -1 : 0;
+}
+
+static long ref_partition_base(int pivot, int * A, long lo, long hi, const int * key)
+{
+	long s = lo, e = hi;
+	for (;;) {
+		while (s < e && ref_cmp(A[s], pivot, key) < 0)
+			s++;
+		while (s < e && ref_cmp(A[e], pivot, key) > 0)
+			e--;
+		if (s >= e)
+			break;
+		std::swap(A[s], A[e]);
+		s++;
+		e--;
+	}
+	if (ref_cmp(A[s], pivot, key) < 0)
+		s++;
+	return s;
+}
+
+static long ref_partition_auto(int * A, long lo, long end, const int * key)
+{
+	const long N = end - lo;
+	if (N == 1)
+		return lo;
+	const long hi = end - 1, pv = (lo + hi) / 2;
+	if (ref_cmp(A[lo], A[hi], key) > 0)
+		std::swap(A[lo], A[hi]);
+	if (N == 2)
+		return hi;
+	if (ref_cmp(A[lo], A[pv], key) > 0)
+		std::swap(A[lo], A[pv]);
+	if (ref_cmp(A[pv], A[hi], key) > 0)
+		std::swap(A[pv], A[hi]);
+	if (N == 3)
+		return pv;
+	return ref_partition_base(A[pv], A, lo + 1, hi - 1, key);
+}
+
+static void ref_quicksort(int * A, long N, const int * key)
+{
+	if (N < 2)
+		return;
+	std::vector<long> stack((size_t) N);
+	long s = 0, e = N - 1, i = 0;
+	for (;;) {
+		while (s >= e) {
+			if (s == 0)
+				return;
+			i--;
+			e--;
+			s = stack[(size_t) i];
+		}
+		const long m = ref_partition_auto(A, s, e + 1, key);
+		stack[(size_t) i++] = s;
+		s = m;
+	}
 }
 
 int bits_for64(int64_t v)
@@ -1215,6 +1337,80 @@ int convert_div(Handle & h)
 		return SPMV_ERR_BOUNDS;
 	}
 	h.kernels_per_run = nsplit > 0 ? 2 : 1;
+	if (!h.desc.div_packet_reordering)
+		return SPMV_OK;
+
+	// 11) packet reordering: medians on the GPU, group order on the host, bytes moved on the GPU
+	DevBuf rk, rv, med;
+	SPMV_TRY(rk.alloc(nnz * 8, s));
+	SPMV_TRY(rv.alloc(nnz * 4, s));
+	SPMV_TRY(med.alloc(NP * 8, s));
+	pkt_col_keys_kernel<<<eg, 256, 0, s>>>(pkt_of.as<int32_t>(), h.d_ci, nnz, rk.as<uint64_t>(), rv.as<uint32_t>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	SPMV_TRY(radix_sort_pairs(rk.as<uint64_t>(), rv.as<uint32_t>(), nnz, 32 + bits_for64(NP), s));
+	pkt_median_kernel<<<(unsigned) ceil_div(NP, 256), 256, 0, s>>>(rk.as<uint64_t>(), pk_j.as<int32_t>(),
+			pk_nv.as<int32_t>(), NP, med.as<int64_t>());
+	SPMV_CUDA_TRY(cudaGetLastError());
+	std::vector<int64_t> hmed((size_t) NP), hoff((size_t) NP + 1), hfirst((size_t) T + 1), hgroups((size_t) h.num_group_entries),
+			hbytes((size_t) T), hng((size_t) T);
+	std::vector<uint8_t> hgrp((size_t) NP);
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hmed.data(), med.p, NP * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hoff.data(), h.d_pkt, (NP + 1) * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hfirst.data(), th_first.p, (T + 1) * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hgroups.data(), h.d_groups, h.num_group_entries * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hbytes.data(), h.d_thread_bytes, T * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hng.data(), h.d_thread_groups, T * 8, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaMemcpyAsync(hgrp.data(), pk_grp.p, NP, cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	std::vector<int64_t> plan, new_groups((size_t) h.num_group_entries);
+	int64_t gbase_t = 0, tbase = 0;
+	for (int t = 0; t < T; t++) {
+		const int64_t G = hng[(size_t) t];
+		const int64_t * go = &hgroups[(size_t) gbase_t];        // G + 1 offsets, relative to the thread's stream
+		const int64_t p0 = hfirst[(size_t) t], p1 = hfirst[(size_t) t + 1];
+		std::vector<int> key((size_t) (G > 0 ? G : 1)), rev((size_t) (G > 0 ? G : 1));
+		for (int64_t k = 0; k < G; k++) {
+			key[(size_t) k] = (int) hmed[(size_t) (p0 + k)];        // the median of the thread's k-th packet
+			rev[(size_t) k] = (int) k;
+		}
+		ref_quicksort(rev.data(), (long) G, key.data());
+		std::vector<int64_t> newpos((size_t) G + 1), dest_of((size_t) (G > 0 ? G : 1));
+		int64_t run = 0;
+		for (int64_t k = 0; k < G; k++) {
+			const int64_t g = rev[(size_t) k];
+			newpos[(size_t) k] = run;
+			dest_of[(size_t) g] = run;
+			plan.push_back(tbase + go[g]);
+			plan.push_back(tbase + run);
+			plan.push_back(go[g + 1] - go[g]);
+			run += go[g + 1] - go[g];
+		}
+		newpos[(size_t) G] = run;
+		for (int64_t k = 0; k <= G; k++)
+			new_groups[(size_t) (gbase_t + k)] = newpos[(size_t) k];
+		// every packet moves with its group
+		int64_t g = -1;
+		for (int64_t p = p0; p < p1; p++) {
+			if (hgrp[(size_t) p] || g < 0)
+				g++;
+			hoff[(size_t) p] = tbase + dest_of[(size_t) g] + (hoff[(size_t) p] - tbase - go[g]);
+		}
+		gbase_t += G + 1;
+		tbase += hbytes[(size_t) t];
+	}
+	const int64_t nplan = (int64_t) plan.size() / 3;
+	if (nplan > 0) {
+		DevBuf dplan, old;
+		SPMV_TRY(dplan.alloc(plan.size() * 8, s));
+		SPMV_TRY(old.alloc(total + 16, s));
+		SPMV_CUDA_TRY(cudaMemcpyAsync(dplan.p, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, s));
+		SPMV_CUDA_TRY(cudaMemcpyAsync(old.p, h.d_div, total + 16, cudaMemcpyDeviceToDevice, s));
+		move_groups_kernel<<<(unsigned) nplan, 256, 0, s>>>(old.as<uint8_t>(), h.d_div, dplan.as<int64_t>(), nplan);
+		SPMV_CUDA_TRY(cudaGetLastError());
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_pkt, hoff.data(), (NP + 1) * 8, cudaMemcpyHostToDevice, s));
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_groups, new_groups.data(), h.num_group_entries * 8, cudaMemcpyHostToDevice, s));
+		SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	}
 	return SPMV_OK;
 }
 

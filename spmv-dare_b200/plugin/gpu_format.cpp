@@ -11,7 +11,8 @@
  * Errors keep the reference's behaviour: print and exit (error(), e.g. csr.cpp:131-132).
  *
  * Environment (config.sh:67-159 contract, plus the GPU knobs):
- *   CSRCV_NUM_PACKET_VALS, DIV_VC_TOLERANCE   DIV-RF packet size / lossy tolerance
+ *   CSRCV_NUM_PACKET_VALS, DIV_VC_TOLERANCE, DIV_PACKET_REORDERING   DIV-RF packet size /
+ *                                             lossy tolerance / packet-group order
  *   SPMV_GPU_VEC_LEN, SPMV_GPU_SELLCS_C, SPMV_GPU_SELLCS_SIGMA, SPMV_GPU_EXACT,
  *   SPMV_GPU_BLOCK_NNZ, SPMV_GPU_STAGES, SPMV_GPU_THREADS, SPMV_GPU_KERNEL
  * The thread count that defines the reference layouts is omp_get_max_threads(), as in
@@ -101,6 +102,7 @@ csr_to_format(INT_T * row_ptr, INT_T * col_ind, ValueTypeReference * values, lon
 	d.sellcs_sigma = (int32_t) env_long("SPMV_GPU_SELLCS_SIGMA", d.sellcs_sigma);
 	d.div_packet_vals = (int32_t) env_long("CSRCV_NUM_PACKET_VALS", d.div_packet_vals);
 	d.div_tolerance = env_double("DIV_VC_TOLERANCE", d.div_tolerance);
+	d.div_packet_reordering = (int32_t) env_long("DIV_PACKET_REORDERING", 0);
 	d.exact = (int32_t) env_long("SPMV_GPU_EXACT", d.exact);
 	d.block_nnz = (int32_t) env_long("SPMV_GPU_BLOCK_NNZ", 0);
 	d.stages = (int32_t) env_long("SPMV_GPU_STAGES", 0);

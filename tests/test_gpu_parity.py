@@ -440,6 +440,55 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
 
 
+@pytest.mark.parametrize("pv,threads,L", [(16384, 8, 4), (1000, 8, 4), (64, 3, 4), (512, 5, 32)])
+def test_div_rf_packet_reordering_matches_reference(sb, orc, pv, threads, L, monkeypatch):
+    """DIV_PACKET_REORDERING=1 (div.cpp:377-395, :455-498): packet bytes and packet-group
+    offsets bit for bit against the reference compiled from its sources, with the same
+    setting, on every golden case (small packets: many groups per thread, long rows split
+    across packets, equal medians); y within 1e-12 and equal to the unordered layout's."""
+    if not orc.ref_available("div_rf"):
+        pytest.fail("the compiled reference for div_rf is missing (make -C oracle ref)")
+    monkeypatch.setenv("DIV_PACKET_REORDERING", "1")
+    monkeypatch.setenv("CSRCV_NUM_PACKET_VALS", str(pv))
+    for name in golden_names():
+        g = load_golden(name)
+        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+        continue_ref = L == 4        # the reference's x86 build has VEC_LEN = 4
+        mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=L, div_packet_vals=pv, div_packet_reordering=1)
+        if continue_ref:
+            R = orc.RefFormat("div_rf", rp, ci, v, n=int(g["n"]), threads=threads)
+            try:
+                a = R.div_arrays()
+            finally:
+                R.close()
+            assert np.array_equal(mf.export("div_data"), orc.div_zero_header_padding(a["data"], L)), name
+            assert np.array_equal(mf.export("div_groups"), a["group_pos"]), name
+        y = mf.spmv(x, np.full(mf.m, 1.0))
+        gold, absy = orc.csr_gold(rp, ci, v, x)
+        assert rel_row_error(y, gold, absy) <= TOL
+        plain = _mk(sb, g, "div_rf", num_threads=threads, vec_len=L, div_packet_vals=pv)
+        assert plain.export("div_data").size == mf.export("div_data").size
+        assert rel_row_error(plain.spmv(x, np.full(mf.m, 1.0)), y, absy) <= TOL
+
+
+def test_div_rf_reordering_config1(sb, orc, monkeypatch):
+    """The 100k-row configuration with reordering, against the compiled reference."""
+    if not orc.ref_available("div_rf"):
+        pytest.fail("the compiled reference for div_rf is missing (make -C oracle ref)")
+    monkeypatch.setenv("DIV_PACKET_REORDERING", "1")
+    monkeypatch.setenv("CSRCV_NUM_PACKET_VALS", "16384")
+    gm = sb.generate_artificial(100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14)
+    rp, ci, v = gm.row_ptr, gm.col_ind, 2.0 * gm.values - 1.0
+    mf = sb.csr_to_format(rp, ci, v, format="div_rf", div_packet_reordering=1)
+    R = orc.RefFormat("div_rf", rp, ci, v, threads=T)
+    try:
+        a = R.div_arrays()
+    finally:
+        R.close()
+    assert np.array_equal(mf.export("div_data"), orc.div_zero_header_padding(a["data"], V))
+    assert np.array_equal(mf.export("div_groups"), a["group_pos"])
+
+
 @pytest.mark.parametrize("tol", [1e-6, 1e-3])
 def test_div_rf_lossy_values(sb, orc, tol):
     """DIV_VC_TOLERANCE: rounded values, same bytes as the restatement, relative value
