@@ -73,6 +73,10 @@ extern "C" {
  *   div_packet_reordering DIV_PACKET_REORDERING (config.sh:133): each thread's packet
  *                        groups stored in ascending order of a median column
  *                        (div.cpp:377-395, :455-498).                            default 0
+ *   pack_cols            FP32 variant: 1 = the kernel reads a device copy of the column
+ *                        indices packed per staged block (smallest column + a fixed bit
+ *                        width), 0 = plain int32 columns.  Values and the exported
+ *                        arrays are unchanged.                                   default 0
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,
@@ -132,7 +136,8 @@ typedef struct spmv_format_desc {
 	int32_t wait_limit_us;
 	int32_t debug_flags;
 	int32_t div_packet_reordering;
-	int32_t reserved[3];
+	int32_t pack_cols;
+	int32_t reserved[2];
 } spmv_format_desc;
 
 #define SPMV_DEBUG_WITHHOLD_HANDOFF 1

@@ -81,6 +81,14 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "wait_limit_us must be in [0, 60e6] (got %d)", d.wait_limit_us);
 		return SPMV_ERR_ARG;
 	}
+	if (d.pack_cols != 0 && d.pack_cols != 1) {
+		set_error(SPMV_ERR_ARG, "pack_cols must be 0 or 1 (got %d)", d.pack_cols);
+		return SPMV_ERR_ARG;
+	}
+	if (d.pack_cols == 1 && d.values != SPMV_VALUES_F32) {
+		set_error(SPMV_ERR_ARG, "pack_cols applies to the FP32 variant");
+		return SPMV_ERR_ARG;
+	}
 	if (d.div_packet_reordering != 0 && d.div_packet_reordering != 1) {
 		set_error(SPMV_ERR_ARG, "div_packet_reordering must be 0 or 1 (got %d)", d.div_packet_reordering);
 		return SPMV_ERR_ARG;

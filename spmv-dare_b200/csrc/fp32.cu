@@ -201,7 +201,39 @@ struct F32WsArgs {
 	int * err;
 	long long wait_budget;   // bound of the kernel's waits, clock cycles
 	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
+	const int4 * pinfo;      // packed columns: per block {16-byte offset, base, bits, stream bytes}
+	const uint32_t * pcols;  // packed columns: the streams (pack.cu)
 };
+
+// Column of entry e of a packed block stream (pack.cu): two whole words and a funnel shift.
+__device__ __forceinline__ int32_t packed_col(const uint32_t * words, int e, int bits, int32_t base)
+{
+	const uint32_t bit = (uint32_t) e * (uint32_t) bits;
+	const uint32_t w = bit >> 5;
+	const uint32_t v = __funnelshift_r(words[w], words[w + 1], bit & 31);
+	return base + (int32_t) (bits >= 32 ? v : (v & ((1u << bits) - 1u)));
+}
+
+// Packed variant: the stage holds values | x, and the block's packed column stream is copied
+// to the top of the x region, so that x of stage position p only overwrites stream words
+// of entries below p + 1 (x at byte 4p, the stream at 4 cap - bytes + e * bits / 8).
+__device__ __forceinline__ void f32ws_issue_packed(const F32WsArgs & a, const StagedBlock & d, const int4 & pi, int s,
+		uint8_t * smem, uint64_t * bars)
+{
+	if (d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	uint8_t * st = smem + (size_t) s * a.stage_bytes;
+	uint8_t * words = st + (size_t) a.cap_al * 8 - (size_t) pi.w;
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 4u + (uint32_t) pi.w);
+	bulk_g2s(st, a.vals + e0, cnt * 4u, &bars[s]);
+	bulk_g2s(words, a.pcols + (int64_t) pi.x * 4, (uint32_t) pi.w, &bars[s]);
+}
 
 __device__ __forceinline__ void f32ws_issue(const F32WsArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
 {
@@ -220,10 +252,12 @@ __device__ __forceinline__ void f32ws_issue(const F32WsArgs & a, const StagedBlo
 	bulk_g2s(sc, a.cols + e0, cnt * 4u, &bars[s]);
 }
 
+template <bool PACKED>
 __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
 	__shared__ StagedBlock sdesc[8];
+	__shared__ int4 spack[8];
 	const int S = a.stages;
 	uint64_t * full = reinterpret_cast<uint64_t *>(smem + (size_t) S * a.stage_bytes);
 	uint64_t * prod = full + S;
@@ -245,13 +279,39 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 		const int gt = threadIdx.x;
 		for (int64_t b = b_begin; b < b_end; b++) {
 			const bool ok = mbar_wait_bounded(&full[s], parity, a.wait_budget);
-			if (!__all_sync(0xffffffffu, ok)) {            // the warp leaves together
-				if ((gt & 31) == 0)
+			if (named_bar_or(2, ng, !ok)) {                // the gather warps leave together
+				if (gt == 0)
 					dev_flag_error(a.err, DEV_ERR_TIMEOUT);
 				return;
 			}
 			const StagedBlock d = sdesc[s];
-			if (d.elems > 0) {
+			if (PACKED && d.elems > 0) {
+				// rounds of WS_GATHER_SLOTS * ng consecutive entries, the same count for every
+				// gather thread: a round's x is stored only once every gather thread has
+				// decoded the round's columns (named barrier 2), since x may overwrite them
+				uint8_t * st = smem + (size_t) s * a.stage_bytes;
+				float * xg = reinterpret_cast<float *>(st + (size_t) a.cap_al * 4);
+				const int4 pi = spack[s];
+				const uint32_t * words = reinterpret_cast<const uint32_t *>(st + (size_t) a.cap_al * 8 - (size_t) pi.w);
+				const int off = d.elem0 & 3;
+				const int per_round = WS_GATHER_SLOTS * ng;
+				for (int rb = 0; rb < d.elems; rb += per_round) {
+					float xv[WS_GATHER_SLOTS];
+					#pragma unroll
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
+						const int e = rb + gt + k * ng;
+						if (e < d.elems)
+							xv[k] = __ldg(a.x + packed_col(words, e, pi.z, pi.y));
+					}
+					named_bar_sync(2, ng);
+					#pragma unroll
+					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
+						const int e = rb + gt + k * ng;
+						if (e < d.elems)
+							xg[off + e] = xv[k];
+					}
+				}
+			} else if (d.elems > 0) {
 				uint8_t * st = smem + (size_t) s * a.stage_bytes;
 				int32_t * sc = reinterpret_cast<int32_t *>(st + (size_t) a.cap_al * 4);
 				float * xg = reinterpret_cast<float *>(sc);     // x of entry e replaces its column
@@ -290,7 +350,13 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 			if (b < b_end) {
 				const StagedBlock d = a.blocks[b];
 				sdesc[q] = d;
-				f32ws_issue(a, d, q, smem, full);
+				if (PACKED) {
+					const int4 pi = a.pinfo[b];
+					spack[q] = pi;
+					f32ws_issue_packed(a, d, pi, q, smem, full);
+				} else {
+					f32ws_issue(a, d, q, smem, full);
+				}
 			}
 		}
 	named_bar_sync(1, nr);
@@ -298,8 +364,12 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 	for (int64_t b = b_begin; b < b_end; b++) {
 		const int64_t nb = b + S;
 		StagedBlock dnext{};
-		if (rt == 0 && nb < b_end)
+		int4 pnext{};
+		if (rt == 0 && nb < b_end) {
 			dnext = a.blocks[nb];
+			if (PACKED)
+				pnext = a.pinfo[nb];
+		}
 		const StagedBlock d = sdesc[s];
 		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
 		int js = 0, je = 0;
@@ -344,7 +414,12 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 		named_bar_sync(1, nr);
 		if (rt == 0 && nb < b_end) {
 			sdesc[s] = dnext;
-			f32ws_issue(a, dnext, s, smem, full);
+			if (PACKED) {
+				spack[s] = pnext;
+				f32ws_issue_packed(a, dnext, pnext, s, smem, full);
+			} else {
+				f32ws_issue(a, dnext, s, smem, full);
+			}
 		}
 		if (++s == S) {
 			s = 0;
@@ -690,9 +765,9 @@ __global__ void conv_kernel_f2d(const float * in, double * out, int64_t n)
 
 }  // namespace
 
-const void * ws_f32_kernel_fn()
+const void * ws_f32_kernel_fn(bool packed)
 {
-	return (const void *) ws_f32_kernel;
+	return packed ? (const void *) ws_f32_kernel<true> : (const void *) ws_f32_kernel<false>;
 }
 
 int f32ws_stage_bytes(int cap_al)
@@ -781,6 +856,8 @@ int convert_f32(Handle & h)
 		h.desc = saved;
 		if (st != SPMV_OK)
 			return st;
+		if (h.desc.pack_cols == 1)
+			SPMV_TRY(build_packed_cols(h));
 		h.kernels_per_run = h.num_blocks > 0 ? 1 : 0;
 		return SPMV_OK;
 	}
@@ -865,7 +942,12 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 		w.err = h.d_err;
 		w.wait_budget = wait_budget_cycles(h.desc.wait_limit_us);
 		w.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
-		ws_f32_kernel<<<h.grid, h.threads, h.smem_bytes, s>>>(w);
+		w.pinfo = h.d_pinfo;
+		w.pcols = h.d_pcols;
+		if (h.d_pcols)
+			ws_f32_kernel<true><<<h.grid, h.threads, h.smem_bytes, s>>>(w);
+		else
+			ws_f32_kernel<false><<<h.grid, h.threads, h.smem_bytes, s>>>(w);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}

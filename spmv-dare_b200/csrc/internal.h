@@ -108,6 +108,9 @@ struct Handle {
 	int2 * d_items = nullptr;    // kernel 10: work items (slice ranges), heaviest first
 	int64_t num_items = 0;
 	unsigned int * d_queue = nullptr;  // kernel 10: work-queue head and finished-warp count
+	int4 * d_pinfo = nullptr;    // packed columns: per block {16-byte offset, base, bits, bytes}
+	uint32_t * d_pcols = nullptr;  // packed columns: the block streams
+	int64_t packed_bytes = 0;
 
 	// warp-autonomous kernel
 	WarpChunk * d_chunks = nullptr;
@@ -193,7 +196,8 @@ int convert_sell(Handle & h, bool sorted);
 int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
 int convert_f32(Handle & h);
-const void * ws_f32_kernel_fn();   // the FP32 warp-specialised kernel (geometry queries)
+const void * ws_f32_kernel_fn(bool packed);   // the FP32 warp-specialised kernel (geometry queries)
+int build_packed_cols(Handle & h);  // packed column streams of the staged blocks (pack.cu)
 int f32ws_stage_bytes(int cap_al);  // its stage size: 8 bytes per staged entry
 int run_mixed_noalloc(Handle & h, const double * d_x, double * d_y, cudaStream_t s);
 int convert_vector_d2f(const double * in, float * out, int64_t n, cudaStream_t s);

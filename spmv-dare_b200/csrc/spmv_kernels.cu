@@ -1374,7 +1374,7 @@ int staged_geometry(Handle & h)
 			h.stages = 2;
 		h.smem_bytes = (size_t) h.stages * stage_bytes + (size_t) h.stages * 16;
 		// FP32-value handles run ws_f32_kernel (fp32.cu), whose stage is also 12 B per entry
-		const void * kern = (h.desc.values == SPMV_VALUES_F32) ? ws_f32_kernel_fn()
+		const void * kern = (h.desc.values == SPMV_VALUES_F32) ? ws_f32_kernel_fn(h.desc.pack_cols == 1)
 		                    : (const void *) (h.exec_kernel == 8 ? pick_ws_tiled(h) : pick_ws(h));
 		if (!kern) {
 			set_error(SPMV_ERR_ARG, "no warp-specialised kernel for format %d with vec_len %d", h.desc.format,

@@ -48,6 +48,31 @@ def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
     assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
 
 
+@pytest.mark.parametrize("block_nnz", [0, 256, 3072])
+def test_fp32_packed_columns_match_dot2_oracle(sb, orc, block_nnz):
+    """pack_cols=1: the kernel reads the column indices packed per staged block (smallest
+    column + a fixed bit width; 1-bit to 31-bit fields, long rows as chunk runs); y is the
+    sequential Dot2 oracle's bit for bit on every golden case and on a matrix whose blocks
+    need every field width from 0 to 22 bits."""
+    cases = [load_golden(n) for n in golden_names()]
+    rng = np.random.default_rng(21)
+    m, n = 3000, 4000000
+    lens = rng.integers(0, 60, m)
+    lens[::97] = rng.integers(500, 5000, lens[::97].size)
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    spans = 2 ** rng.integers(0, 23, m)
+    ci = np.concatenate([np.sort(rng.integers(0, max(1, min(n, s)), k)) + rng.integers(0, n - min(n, s) + 1)
+                         for k, s in zip(lens, spans)]).astype(np.int32)
+    cases.append(dict(row_ptr=rp, col_ind=ci, values=rng.uniform(-1, 1, ci.size), x=rng.uniform(-1, 1, n)))
+    for g in cases:
+        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+        mf, y32, y64 = _run(sb, rp, ci, v, x, pack_cols=1, block_nnz=block_nnz)
+        ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
+        assert np.array_equal(y32.view(np.uint32), ref.view(np.uint32)), (rp.size - 1, block_nnz)
+        assert np.array_equal(y64.astype(np.float32).view(np.uint32), y32.view(np.uint32))
+        assert np.array_equal(mf.export("col_ind"), ci)
+
+
 @pytest.mark.parametrize("kernel", [7, -1])
 @pytest.mark.parametrize("case", ["long_rows", "empty_rows", "chunk_multiple", "one_long_row"])
 def test_fp32_segmented_kernel_edge_cases(sb, orc, case, kernel):
