@@ -365,6 +365,38 @@ void spmv_mtx_destroy(spmv_mtx * mtx);
 int spmv_coo_to_csr_device(const int32_t * d_rows, const int32_t * d_cols, const double * d_vals, int64_t m,
 		int64_t n, int64_t nnz, int32_t * d_row_ptr, int32_t * d_col_ind, double * d_values, void * stream);
 
+/* ---------------------------------------------------------------- symmetric matrices, RCM */
+/*
+ * The bench's symmetric transforms on the GPU (host CSR in, host CSR out through an opaque
+ * result; NULL + *status on error):
+ *   spmv_expand_symmetric  csr_expand_symmetric (lib/storage_formats/csr/csr_gen.c:256-336)
+ *                          with sorted columns: a stored lower triangle to the full matrix
+ *                          (an entry above the diagonal is SPMV_ERR_CSR, as the reference
+ *                          stops on it);
+ *   spmv_drop_upper        csr_drop_upper (csr_gen.c:344-420) with sorted columns;
+ *   spmv_rcm               the bench's rcm() (src/bench.cpp:280-358): reverse Cuthill-McKee
+ *                          (lib/rcm/rcm_gen.c:96-410) with sorted columns, of the full matrix
+ *                          (symmetry_expanded = 1) or of a stored triangle (0: expanded first,
+ *                          its upper triangle dropped after).  permutation[old row] = new row.
+ * RCM ordering: the degree <= 1 vertices first in vertex order, then frontier by frontier
+ * ordered by (earliest visited neighbour, degree, index), new components at the unvisited
+ * vertex of least (degree, index); the reference places the degree <= 1 vertices through an
+ * atomic counter, so the permutations agree with its one-thread run.
+ */
+typedef struct spmv_csr_out spmv_csr_out;
+spmv_csr_out * spmv_expand_symmetric(const int32_t * row_ptr, const int32_t * col_ind, const double * values,
+		int64_t m, int64_t n, int64_t nnz, int * status);
+spmv_csr_out * spmv_drop_upper(const int32_t * row_ptr, const int32_t * col_ind, const double * values, int64_t m,
+		int64_t n, int64_t nnz, int * status);
+spmv_csr_out * spmv_rcm(const int32_t * row_ptr, const int32_t * col_ind, const double * values, int64_t m, int64_t n,
+		int64_t nnz, int32_t symmetry_expanded, int * status);
+int spmv_csr_out_info(const spmv_csr_out * out, int64_t * m, int64_t * n, int64_t * nnz, int64_t * nnz_diag);
+/* row_ptr int32[m+1], col_ind int32[nnz], values f64[nnz], permutation int32[m] (RCM only);
+ * any may be NULL. */
+int spmv_csr_out_get(const spmv_csr_out * out, int32_t * row_ptr, int32_t * col_ind, double * values,
+		int32_t * permutation);
+void spmv_csr_out_destroy(spmv_csr_out * out);
+
 /* Library version string. */
 const char * spmv_version(void);
 

@@ -302,6 +302,15 @@ def _ref(name):
             L.ref_gen_free.argtypes = [c_void_p]
             L.ref_cross_row_similarity.restype = c_double
             L.ref_cross_row_similarity.argtypes = [c_void_p, c_void_p, c_long, c_long, c_long, c_int]
+        elif name == "rcm":
+            L.ref_sym_transform.restype = c_void_p
+            L.ref_sym_transform.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_long, c_long, c_long, c_long, c_int]
+            L.ref_sym_nnz.restype = c_long
+            L.ref_sym_nnz.argtypes = [c_void_p]
+            L.ref_sym_nnz_diag.restype = c_long
+            L.ref_sym_nnz_diag.argtypes = [c_void_p]
+            L.ref_sym_arrays.argtypes = [c_void_p] * 5
+            L.ref_sym_free.argtypes = [c_void_p]
         elif name == "mtx":
             L.ref_mtx_import.restype = c_void_p
             L.ref_mtx_import.argtypes = [c_char_p, c_long, c_int]
@@ -451,6 +460,27 @@ def ref_read_mtx(path, expand_symmetry=True, threads=4):
         L.ref_mtx_free(h)
     return dict(row_ptr=rp, col_ind=ci[:nnz], values=v[:nnz], m=m, n=n, nnz=nnz, nnz_diag=int(info[3]),
                 nnz_non_diag=int(info[4]), symmetric=int(info[5]), expanded=int(info[6]))
+
+
+def ref_sym_transform(kind, rp, ci, v, n=None, expanded=1, threads=1):
+    """The reference's csr_expand_symmetric (kind "expand"), csr_drop_upper ("drop") or the
+    bench's rcm() ("rcm"): (row_ptr, col_ind, values, permutation or None, nnz_diag)."""
+    L = _ref("rcm")
+    rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), _c(v, np.float64)
+    m = rp.size - 1
+    k = {"expand": 0, "drop": 1, "rcm": 2}[kind]
+    h = L.ref_sym_transform(k, _p(rp), _p(ci), _p(v), m, m if n is None else n, int(rp[-1]), expanded, threads)
+    try:
+        nnz = L.ref_sym_nnz(h)
+        orp = np.zeros(m + 1, np.int32)
+        oci = np.zeros(max(nnz, 1), np.int32)
+        ov = np.zeros(max(nnz, 1), np.float64)
+        perm = np.zeros(max(m, 1), np.int32)
+        L.ref_sym_arrays(h, _p(orp), _p(oci), _p(ov), _p(perm) if k == 2 else None)
+        nd = L.ref_sym_nnz_diag(h)
+    finally:
+        L.ref_sym_free(h)
+    return orp, oci[:nnz], ov[:nnz], (perm[:m] if k == 2 else None), nd
 
 
 def ref_sellcs_convert(rp, ci, v, C, sigma):

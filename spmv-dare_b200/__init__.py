@@ -30,7 +30,7 @@ from ._capi import FORMATS, VALUES_F32, VALUES_F64
 __all__ = [
     "SpmvError", "Matrix_Format", "csr_to_format", "statistics_print_labels", "generate_artificial",
     "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version", "Batch", "read_mtx", "MtxMatrix",
-    "coo_to_csr",
+    "coo_to_csr", "expand_symmetric", "drop_upper", "rcm",
 ]
 
 
@@ -471,3 +471,47 @@ def coo_to_csr(rows, cols, values, m, n):
     if st:
         _raise(st)
     return rp, ci[:nnz], vv[:nnz]
+
+
+def _csr_out(fn, row_ptr, col_ind, values, n, *extra):
+    lib = library()
+    rp, ci, vv = _host(row_ptr, np.int32), _host(col_ind, np.int32), _host(values, np.float64)
+    m = rp.size - 1
+    st = c_int(0)
+    o = fn(rp.ctypes.data, ci.ctypes.data if ci.size else None, vv.ctypes.data if vv.size else None, m, int(n),
+           int(rp[-1]), *extra, byref(st))
+    if not o:
+        _raise(st.value)
+    try:
+        mm, nn, nz, nd = c_int64(), c_int64(), c_int64(), c_int64()
+        lib.spmv_csr_out_info(o, byref(mm), byref(nn), byref(nz), byref(nd))
+        orp = np.empty(mm.value + 1, np.int32)
+        oci = np.empty(max(nz.value, 1), np.int32)
+        ov = np.empty(max(nz.value, 1), np.float64)
+        perm = np.empty(max(mm.value, 1), np.int32)
+        lib.spmv_csr_out_get(o, orp.ctypes.data, oci.ctypes.data, ov.ctypes.data, perm.ctypes.data)
+    finally:
+        lib.spmv_csr_out_destroy(o)
+    return orp, oci[:nz.value], ov[:nz.value], perm[:mm.value], nd.value
+
+
+def expand_symmetric(row_ptr, col_ind, values, n=None):
+    """csr_expand_symmetric (csr_gen.c:256-336) on the GPU: (row_ptr, col_ind, values, nnz_diag)."""
+    rp, ci, v, _, nd = _csr_out(library().spmv_expand_symmetric, row_ptr, col_ind, values,
+                                len(row_ptr) - 1 if n is None else n)
+    return rp, ci, v, nd
+
+
+def drop_upper(row_ptr, col_ind, values, n=None):
+    """csr_drop_upper (csr_gen.c:344-420) on the GPU: (row_ptr, col_ind, values, nnz_diag)."""
+    rp, ci, v, _, nd = _csr_out(library().spmv_drop_upper, row_ptr, col_ind, values,
+                                len(row_ptr) - 1 if n is None else n)
+    return rp, ci, v, nd
+
+
+def rcm(row_ptr, col_ind, values, symmetry_expanded=True):
+    """The bench's rcm() (src/bench.cpp:280-358) on the GPU: (row_ptr, col_ind, values,
+    permutation), permutation[old row] = new row."""
+    rp, ci, v, perm, _ = _csr_out(library().spmv_rcm, row_ptr, col_ind, values, len(row_ptr) - 1,
+                                  1 if symmetry_expanded else 0)
+    return rp, ci, v, perm

@@ -116,6 +116,12 @@ SIGNATURES = {
     "spmv_mtx_destroy": (None, [c_void_p]),
     "spmv_coo_to_csr_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p, c_void_p,
                                        c_void_p, c_void_p]),
+    "spmv_expand_symmetric": (c_void_p, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, POINTER(c_int)]),
+    "spmv_drop_upper": (c_void_p, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, POINTER(c_int)]),
+    "spmv_rcm": (c_void_p, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int32, POINTER(c_int)]),
+    "spmv_csr_out_info": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_csr_out_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_csr_out_destroy": (None, [c_void_p]),
 }
 
 _lib = None

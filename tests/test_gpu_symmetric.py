@@ -1,0 +1,112 @@
+"""Symmetric matrices: the bench's transforms on the GPU against the reference's own code
+(oracle/_ref/libref_rcm.so: csr_expand_symmetric, csr_drop_upper, and rcm() of
+src/bench.cpp:280-358 with reverse_cuthill_mckee, lib/rcm/rcm_gen.c:96-410).
+
+The reference places the degree <= 1 vertices through an atomic counter shared by its
+threads, so its permutation changes with the thread schedule; it is pinned here at one
+thread, where that order is the vertex order the GPU uses.  Bars: every array bit for bit
+(row_ptr, col_ind, values, permutation, nnz_diag).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.uint64)
+
+
+def _lower(m, seed, band=200, max_per_row=6, isolated=0, diag=True):
+    """A random lower triangle (sorted columns): rows within `band` of the diagonal, some
+    rows left empty so the graph has isolated vertices and several components."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    empty = set(rng.choice(m, isolated, replace=False).tolist()) if isolated else set()
+    for i in range(m):
+        if i in empty:
+            continue
+        js = set(rng.integers(max(0, i - band), i + 1, int(rng.integers(0, max_per_row))).tolist())
+        if diag and rng.uniform() < 0.7:
+            js.add(i)
+        js = [j for j in js if j not in empty]
+        rows += [i] * len(js)
+        cols += sorted(js)
+    rows, cols = np.array(rows, np.int64), np.array(cols, np.int64)
+    rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=m))]).astype(np.int32)
+    return rp, cols.astype(np.int32), rng.uniform(-1, 1, cols.size)
+
+
+CASES = [dict(m=3000, seed=5), dict(m=5000, seed=6, band=20, isolated=300), dict(m=2000, seed=7, band=2000),
+         dict(m=1500, seed=8, band=3, max_per_row=2), dict(m=400, seed=9, diag=False, isolated=50)]
+
+
+def _need(orc):
+    if not orc.ref_available("rcm"):
+        pytest.fail("reference build (oracle/_ref/libref_rcm.so) missing")
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_expand_and_drop_match_reference(sb, orc, case):
+    _need(orc)
+    rp, ci, v = _lower(**CASES[case])
+    erp, eci, ev, end_ = sb.expand_symmetric(rp, ci, v)
+    r = orc.ref_sym_transform("expand", rp, ci, v)
+    assert np.array_equal(erp, r[0]) and np.array_equal(eci, r[1]) and np.array_equal(_bits(ev), _bits(r[2]))
+    assert end_ == r[4]
+    drp, dci, dv, dnd = sb.drop_upper(erp, eci, ev)
+    r = orc.ref_sym_transform("drop", erp, eci, ev)
+    assert np.array_equal(drp, r[0]) and np.array_equal(dci, r[1]) and np.array_equal(_bits(dv), _bits(r[2]))
+    assert np.array_equal(drp, rp) and np.array_equal(dci, ci) and dnd == r[4]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("expanded", [0, 1])
+def test_rcm_matches_reference(sb, orc, case, expanded):
+    _need(orc)
+    rp, ci, v = _lower(**CASES[case])
+    if expanded:
+        rp, ci, v, _ = sb.expand_symmetric(rp, ci, v)
+    grp, gci, gv, gperm = sb.rcm(rp, ci, v, symmetry_expanded=bool(expanded))
+    r = orc.ref_sym_transform("rcm", rp, ci, v, expanded=expanded, threads=1)
+    assert np.array_equal(gperm, r[3]), "permutation differs"
+    assert np.array_equal(grp, r[0]) and np.array_equal(gci, r[1]) and np.array_equal(_bits(gv), _bits(r[2]))
+    m = rp.size - 1
+    assert np.array_equal(np.sort(gperm), np.arange(m))
+
+
+def test_rcm_reduces_bandwidth_and_feeds_every_format(sb, orc):
+    """A scrambled banded matrix: RCM brings its bandwidth back down, and the reordered
+    matrix converts and multiplies in every format like csr_naive does."""
+    _need(orc)
+    rp, ci, v = _lower(4000, 11, band=8)
+    full = sb.expand_symmetric(rp, ci, v)[:3]
+    m = rp.size - 1
+    p = np.random.default_rng(1).permutation(m).astype(np.int32)
+    rows = np.repeat(np.arange(m), np.diff(full[0]))
+    R, C = p[rows], p[full[1]]
+    order = np.lexsort((C, R))
+    srp = np.concatenate([[0], np.cumsum(np.bincount(R, minlength=m))]).astype(np.int32)
+    sci, sv = C[order].astype(np.int32), full[2][order]
+    bw = lambda a, c: int(np.max(np.abs(np.repeat(np.arange(m), np.diff(a)) - c)))
+    nrp, nci, nv, perm = sb.rcm(srp, sci, sv, symmetry_expanded=True)
+    assert bw(nrp, nci) < bw(srp, sci) / 10
+    x = np.random.default_rng(2).uniform(-1, 1, m)
+    ref = orc.csr_spmv(nrp, nci, nv, x)
+    gold, absy = orc.csr_gold(nrp, nci, nv, x)
+    for fmt in ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s", "div_rf"]:
+        y = sb.csr_to_format(nrp, nci, nv, format=fmt).spmv(x, np.full(m, 1.0))
+        if fmt == "csr_naive":
+            assert np.array_equal(_bits(y), _bits(ref))
+        den = np.maximum(np.abs(gold), absy)
+        assert np.max(np.abs(y - gold) / np.where(den > 0, den, 1)) <= 1e-12, fmt
+
+
+def test_transform_errors(sb):
+    rp = np.array([0, 1, 2], np.int32)
+    with pytest.raises(sb.SpmvError) as e:            # an entry above the diagonal
+        sb.expand_symmetric(rp, np.array([1, 1], np.int32), np.ones(2))
+    assert e.value.status == 2
+    with pytest.raises(sb.SpmvError) as e:            # RCM of a rectangular matrix
+        sb._csr_out(sb.library().spmv_rcm, rp, np.array([0, 2], np.int32), np.ones(2), 3, 1)
+    assert e.value.status == 1
