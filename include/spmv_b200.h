@@ -397,6 +397,31 @@ int spmv_csr_out_get(const spmv_csr_out * out, int32_t * row_ptr, int32_t * col_
 		int32_t * permutation);
 void spmv_csr_out_destroy(spmv_csr_out * out);
 
+/* ---------------------------------------------------------------- artificial matrices on the GPU */
+/*
+ * The same generator on the GPU (one thread per anchor segment: the reference reseeds with
+ * seed + row at every anchor row, so segments are independent), into device memory on
+ * `stream`.  The steps and the random stream are the host generator's; CUDA's log, cos,
+ * exp, pow and sqrt may differ from glibc's in the last bit, so a value that lands on a
+ * rounding or rejection boundary can differ: the matrices follow the reference's
+ * distribution, and nearly always match it entry for entry.  Values are U[0,1).
+ * spmv_gen_copy_device copies row_ptr int32[rows+1], col_ind int32[nnz], values f64[nnz]
+ * (any may be NULL) into caller device arrays.
+ */
+typedef struct spmv_gen spmv_gen;
+spmv_gen * spmv_gen_create_device(int64_t rows, int64_t cols, double avg_nnz_per_row, double std_nnz_per_row,
+		const char * distribution, const char * placement, double bw, double skew, double avg_num_neighbours,
+		double cross_row_similarity, uint32_t seed, void * stream, int * status);
+int spmv_gen_info(const spmv_gen * gen, int64_t * m, int64_t * n, int64_t * nnz);
+int spmv_gen_copy_device(const spmv_gen * gen, int32_t * d_row_ptr, int32_t * d_col_ind, double * d_values, void * stream);
+void spmv_gen_destroy(spmv_gen * gen);
+/* The GPU generator's per-segment code run on the host (host libm) into host arrays
+ * (row_ptr[rows+1]; col_ind / values of cap entries); returns nnz or -1.  It checks that
+ * code against spmv_artgen_create without a GPU. */
+int64_t spmv_gen_host_check(int64_t rows, int64_t cols, double avg_nnz_per_row, double std_nnz_per_row,
+		const char * distribution, const char * placement, double bw, double skew, double avg_num_neighbours,
+		double cross_row_similarity, uint32_t seed, int32_t * row_ptr, int32_t * col_ind, double * values, int64_t cap);
+
 /* Library version string. */
 const char * spmv_version(void);
 

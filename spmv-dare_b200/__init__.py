@@ -30,7 +30,7 @@ from ._capi import FORMATS, VALUES_F32, VALUES_F64
 __all__ = [
     "SpmvError", "Matrix_Format", "csr_to_format", "statistics_print_labels", "generate_artificial",
     "ArtificialMatrix", "FORMATS", "format_defaults", "library", "version", "Batch", "read_mtx", "MtxMatrix",
-    "coo_to_csr", "expand_symmetric", "drop_upper", "rcm",
+    "coo_to_csr", "expand_symmetric", "drop_upper", "rcm", "generate_artificial_device",
 ]
 
 
@@ -515,3 +515,33 @@ def rcm(row_ptr, col_ind, values, symmetry_expanded=True):
     rp, ci, v, perm, _ = _csr_out(library().spmv_rcm, row_ptr, col_ind, values, len(row_ptr) - 1,
                                   1 if symmetry_expanded else 0)
     return rp, ci, v, perm
+
+
+def generate_artificial_device(rows, cols, avg_nnz_per_row, std_nnz_per_row, distribution, placement, avg_bw, skew,
+                               avg_num_neighbours, cross_row_similarity, seed, device="cuda", stream=None):
+    """The artificial generator run on the GPU (one thread per anchor segment): CUDA int32
+    row_ptr / col_ind and float64 values (U[0,1)) tensors on `device`."""
+    import torch
+
+    lib = library()
+    dev = torch.device(device)
+    s = _torch_stream(dev, stream)
+    st = c_int(0)
+    g = lib.spmv_gen_create_device(int(rows), int(cols), float(avg_nnz_per_row), float(std_nnz_per_row),
+                                   distribution.encode(), placement.encode(), float(avg_bw), float(skew),
+                                   float(avg_num_neighbours), float(cross_row_similarity), int(seed) & 0xFFFFFFFF, s,
+                                   byref(st))
+    if not g:
+        _raise(st.value)
+    try:
+        m, n, nnz = c_int64(), c_int64(), c_int64()
+        lib.spmv_gen_info(g, byref(m), byref(n), byref(nnz))
+        rp = torch.empty(m.value + 1, dtype=torch.int32, device=dev)
+        ci = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+        v = torch.empty(max(nnz.value, 1), dtype=torch.float64, device=dev)
+        st2 = lib.spmv_gen_copy_device(g, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), s)
+        if st2:
+            _raise(st2)
+    finally:
+        lib.spmv_gen_destroy(g)     # its buffers are freed in stream order, after the copies
+    return rp, ci[:nnz.value], v[:nnz.value]

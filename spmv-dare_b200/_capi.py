@@ -122,6 +122,13 @@ SIGNATURES = {
     "spmv_csr_out_info": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_csr_out_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_csr_out_destroy": (None, [c_void_p]),
+    "spmv_gen_create_device": (c_void_p, [c_int64, c_int64, c_double, c_double, c_char_p, c_char_p, c_double, c_double,
+                                          c_double, c_double, c_uint32, c_void_p, POINTER(c_int)]),
+    "spmv_gen_info": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_gen_copy_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "spmv_gen_destroy": (None, [c_void_p]),
+    "spmv_gen_host_check": (c_int64, [c_int64, c_int64, c_double, c_double, c_char_p, c_char_p, c_double, c_double,
+                                      c_double, c_double, c_uint32, c_void_p, c_void_p, c_void_p, c_int64]),
 }
 
 _lib = None

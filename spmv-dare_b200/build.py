@@ -34,7 +34,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3"
 GCC_FLAGS = ["-O3", "-march=x86-64-v3", "-fPIC", "-fopenmp", "-std=gnu11", "-Wall", "-Wno-unused-result"]
 
 CU_SOURCES = ["primitives.cu", "convert.cu", "spmv_kernels.cu", "warp_kernels.cu", "div.cu", "fp32.cu", "batch.cu", "select.cu",
-              "mtx.cu", "pack.cu", "sym.cu", "api.cu"]
+              "mtx.cu", "pack.cu", "sym.cu", "gen.cu", "api.cu"]
 C_SOURCES = ["artgen.c", "mtx_parse.c"]
 HEADERS = ["common.cuh", "primitives.cuh", "internal.h", "mtx_parse.h"]
 
