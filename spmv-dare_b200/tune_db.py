@@ -34,10 +34,16 @@ def load_package():
 PARAM_KEYS = ["rows", "avg", "std", "skew", "bw", "neigh", "cross"]
 
 
-def to_npz(src, dst, num_classes=24):
+def to_npz(src, dst, num_classes=None):
     """The JSON lines of `src` as compact arrays (sorted by seed; NaN = class not timed,
     inf = class failed)."""
     import numpy as np
+
+    if num_classes is None:
+        load_package()
+        from spmv_dare_b200 import tuning
+
+        num_classes = len(tuning.CLASSES)
 
     R = sorted((json.loads(l) for l in open(src)), key=lambda r: r["seed"])
     times = np.full((len(R), num_classes), np.nan)
@@ -64,6 +70,8 @@ def main(argv=None):
     ap.add_argument("--rows-lo", type=float, default=1e4)
     ap.add_argument("--rows-hi", type=float, default=3e5)
     ap.add_argument("--reps", type=int, default=7)
+    ap.add_argument("--device-gen", action="store_true",
+                    help="generate each matrix on the GPU and convert it from device memory")
     ap.add_argument("--out", required=True)
     a = ap.parse_args(argv)
     import torch
@@ -87,10 +95,17 @@ def main(argv=None):
             if seed in done:
                 continue
             p = workloads.batch_params(seed) if a.set == "batch" else workloads.selector_params(seed, a.rows_lo, a.rows_hi)
-            rp, ci, v, _ = workloads.generate(sb, p)
-            m, n, nnz = rp.size - 1, p["cols"], int(rp[-1])
-            t0 = time.perf_counter()
-            F = selector.features(rp, ci, m, n)
+            if a.device_gen:
+                rp, ci, v = workloads.generate_device(sb, p)
+                m, n, nnz = p["rows"], p["cols"], int(ci.numel())
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                F = selector.features_device(rp, ci, m, n, nnz)
+            else:
+                rp, ci, v, _ = workloads.generate(sb, p)
+                m, n, nnz = rp.size - 1, p["cols"], int(rp[-1])
+                t0 = time.perf_counter()
+                F = selector.features(rp, ci, m, n)
             feat_s = time.perf_counter() - t0
             times, best, cost = tuning.exhaustive(sb, timer, rp, ci, v, m, n, classes, reps=a.reps)
             rec = {"seed": seed, "params": p, "m": m, "n": n, "nnz": nnz, "features": F.tolist(),

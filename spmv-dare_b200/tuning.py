@@ -24,10 +24,13 @@ def _cta(threads, block):
     return {"format": "csr_naive", "kernel": 0, "threads": threads, "block_nnz": block, "stages": 2}
 
 
-# 24 classes: the CSR kernel and its staging geometry (threads, row threads, entries per
+# 29 classes: the CSR kernel and its staging geometry (threads, row threads, entries per
 # block, stages) -- the choice that depends most on the matrix with these kernels -- and
 # the other formats with their own parameters (lanes, slice height, C and sigma), each with
-# the kernel it was timed with in the committed database (data/tune_*.npz).
+# the kernel it is timed with.  New classes are appended, so a database's class indices keep
+# their meaning (of the last five only SELL with 32-row slices adds a batch descriptor to
+# BATCHABLE, below: the others repeat earlier descriptors, or the batch engine does not run
+# the format).
 CLASSES = [
     _ws(160, 64, 768, 3),          # the csr_naive default
     _ws(160, 64, 256, 4),
@@ -53,6 +56,13 @@ CLASSES = [
     {"format": "sell_c_s", "sellcs_c": 64, "sellcs_sigma": 1024, "kernel": 0},
     {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 4},
     {"format": "div_rf"},
+    # the later kernels: SELL-C-sigma on kernels 8 and 10, SELL with 32-row slices on kernel
+    # 10, DIV-RF with 32 lanes (the warp decoder)
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 8},
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 10},
+    {"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 4096, "kernel": 10},
+    {"format": "sell", "vec_len": 32, "kernel": 10},
+    {"format": "div_rf", "vec_len": 32},
 ]
 DEFAULT_CLASS = 0      # what the library picks without a selector
 
@@ -108,7 +118,7 @@ def exhaustive(sb, timer, rp, ci, v, m, n, classes=None, reps=7):
     classes = list(range(len(CLASSES))) if classes is None else list(classes)
     xd = torch.empty(n, dtype=torch.float64, device="cuda").uniform_(-1.0, 1.0)
     yd = torch.empty(m, dtype=torch.float64, device="cuda")
-    nnz = int(rp[-1])
+    nnz = int(ci.numel()) if getattr(ci, "is_cuda", False) else int(rp[-1])
     times = {}
     t0 = time.perf_counter()
     for i in classes:

@@ -50,3 +50,11 @@ def generate(sb, p):
     v = 2.0 * g.values - 1.0
     x = np.random.Generator(np.random.PCG64(p["seed"] + 7919)).uniform(-1.0, 1.0, p["cols"])
     return g.row_ptr, g.col_ind, v, x
+
+
+def generate_device(sb, p):
+    """(row_ptr, col_ind, values) CUDA tensors of the matrix named by p, generated on the GPU
+    (distribution-equivalent to generate(); values mapped v -> 2v - 1)."""
+    rp, ci, v = sb.generate_artificial_device(p["rows"], p["cols"], p["avg"], p["std"], p["distribution"],
+                                              p["placement"], p["bw"], p["skew"], p["neigh"], p["cross"], p["seed"])
+    return rp, ci, 2.0 * v - 1.0
