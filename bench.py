@@ -54,7 +54,8 @@ FALLBACK_HBM = 6650.0
 # that changes the operation order (csr_vec lanes, slice heights) is held to the stated
 # tolerance against csr_naive instead of bit parity.
 TUNED = {
-    "csr_naive": [dict(kernel=4, threads=192, block_rows=64, block_nnz=1024, stages=3),
+    "csr_naive": [dict(pack_cols=1), dict(pack_cols=1, block_nnz=1024),
+                  dict(kernel=4, threads=192, block_rows=64, block_nnz=1024, stages=3),
                   dict(kernel=4, threads=160, block_rows=64, block_nnz=512, stages=3)],
     "csr_vec": [dict(vec_len=8), dict(vec_len=2)],
     "sell": [dict(vec_len=8), dict(vec_len=16), dict(vec_len=32, kernel=10), dict(vec_len=32, kernel=8)],
@@ -834,9 +835,12 @@ def main():
     ap.add_argument("--retune", action="store_true", help="batch: re-run the autotuner instead of its database")
     ap.add_argument("--no-batch", action="store_true", help="leave the batch block out of the default line")
     ap.add_argument("--no-tuned", action="store_true", help="time only the plain settings of each format")
+    ap.add_argument("--params", default="", help="JSON object of descriptor fields for --format (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.params:
+        FORMAT_PARAMS[args.format] = dict(FORMAT_PARAMS.get(args.format, {}), **json.loads(args.params))
     if args.workload == "batch":
         (run_reference_batch if args.impl == "reference" else run_batch)(args)
     elif args.impl == "reference":

@@ -73,10 +73,10 @@ extern "C" {
  *   div_packet_reordering DIV_PACKET_REORDERING (config.sh:133): each thread's packet
  *                        groups stored in ascending order of a median column
  *                        (div.cpp:377-395, :455-498).                            default 0
- *   pack_cols            FP32 variant: 1 = the kernel reads a device copy of the column
- *                        indices packed per staged block (smallest column + a fixed bit
- *                        width), 0 = plain int32 columns.  Values and the exported
- *                        arrays are unchanged.                                   default 0
+ *   pack_cols            csr_naive (FP64 on kernel 4, and the FP32 variant): 1 = the kernel
+ *                        reads a device copy of the column indices packed per staged block
+ *                        (smallest column + a fixed bit width), 0 = plain int32 columns.
+ *                        Values, y and the exported arrays are unchanged.        default 0
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,

@@ -85,8 +85,8 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "pack_cols must be 0 or 1 (got %d)", d.pack_cols);
 		return SPMV_ERR_ARG;
 	}
-	if (d.pack_cols == 1 && d.values != SPMV_VALUES_F32) {
-		set_error(SPMV_ERR_ARG, "pack_cols applies to the FP32 variant");
+	if (d.pack_cols == 1 && d.format != SPMV_FMT_CSR_NAIVE) {
+		set_error(SPMV_ERR_ARG, "pack_cols applies to csr_naive (FP64) and the FP32 variant");
 		return SPMV_ERR_ARG;
 	}
 	if (d.div_packet_reordering != 0 && d.div_packet_reordering != 1) {

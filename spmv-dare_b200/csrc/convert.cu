@@ -565,7 +565,16 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 
 int convert_csr(Handle & h)
 {
-	return build_exec(h, h.d_rp, h.m, 1);
+	SPMV_TRY(build_exec(h, h.d_rp, h.m, 1));
+	if (h.desc.pack_cols == 1) {
+		if (h.exec_kernel != 4) {
+			set_error(SPMV_ERR_ARG, "pack_cols: FP64 csr_naive packs columns for kernel 4 only (got kernel %d)",
+					h.exec_kernel);
+			return SPMV_ERR_ARG;
+		}
+		SPMV_TRY(build_packed_cols(h));
+	}
+	return SPMV_OK;
 }
 
 int convert_sell(Handle & h, bool sorted)

@@ -50,7 +50,18 @@ struct StagedArgs {
 	int * err;
 	long long wait_budget;   // bound of the warp-specialised kernel's waits, clock cycles
 	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
+	const int4 * pinfo;      // packed columns (csr_naive): per block {16-byte offset, base, bits, bytes}
+	const uint32_t * pcols;  // packed columns: the block streams (pack.cu)
 };
+
+// Column of entry e of a packed block stream (pack.cu): two whole words and a funnel shift.
+__device__ __forceinline__ int32_t packed_col64(const uint32_t * words, int e, int bits, int32_t base)
+{
+	const uint32_t bit = (uint32_t) e * (uint32_t) bits;
+	const uint32_t w = bit >> 5;
+	const uint32_t v = __funnelshift_r(words[w], words[w + 1], bit & 31);
+	return base + (int32_t) (bits >= 32 ? v : (v & ((1u << bits) - 1u)));
+}
 
 // Sequential sum of s[0..n) in index order.
 __device__ __forceinline__ double seq_add(const double * s, int n, double sum)
@@ -753,6 +764,25 @@ __device__ __forceinline__ void rows_t(const StagedArgs & a, const StagedBlock &
 // is a run of chunk blocks.  Each CTA walks a contiguous range of the block table.
 // Bulk copy of a block's entries for the warp-specialised kernel (chunk blocks of long
 // units included; only an empty block completes the stage without a copy).
+// Packed variant (csr_naive): the block's packed column stream lands where the columns would.
+__device__ __forceinline__ void ws_issue_packed(const StagedArgs & a, const StagedBlock & d, const int4 & pi, int s,
+		uint8_t * smem, uint64_t * bars)
+{
+	if (d.elems == 0) {
+		mbar_arrive(&bars[s]);
+		return;
+	}
+	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
+	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
+	const uint32_t cnt = (uint32_t) (e1 - e0);
+	double * sv = reinterpret_cast<double *>(smem + (size_t) s * a.stage_bytes);
+	uint8_t * sc = smem + (size_t) s * a.stage_bytes + (size_t) a.cols_off;
+	fence_proxy_async_smem();
+	mbar_arrive_expect_tx(&bars[s], cnt * 8u + (uint32_t) pi.w);
+	bulk_g2s(sv, a.vals + e0, cnt * 8u, &bars[s]);
+	bulk_g2s(sc, a.pcols + (int64_t) pi.x * 4, (uint32_t) pi.w, &bars[s]);
+}
+
 __device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
 {
 	if (d.elems == 0) {
@@ -837,11 +867,12 @@ __device__ __forceinline__ void ws_chunk(const StagedArgs & a, const StagedBlock
 // columns instead of 32 rows x 1 column.  The gather keeps that order (x of stage entry e
 // at e + e / 8) and the row threads walk the tiles (tiled_row).  Blocks start at slice
 // boundaries and chunks at tile boundaries, so off == 0.
-template <Kind K, Arith A, int L, bool YMAP, bool TX = false>
+template <Kind K, Arith A, int L, bool YMAP, bool TX = false, bool PK = false>
 __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 {
 	extern __shared__ __align__(128) uint8_t smem[];
 	__shared__ StagedBlock sdesc[8];
+	__shared__ int4 spack[8];
 	const int S = a.stages;
 	uint64_t * full = reinterpret_cast<uint64_t *>(smem + (size_t) S * a.stage_bytes);
 	uint64_t * prod = full + S;
@@ -875,6 +906,8 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 				const int32_t * sc = reinterpret_cast<const int32_t *>(st + (size_t) a.cols_off);
 				double * xg = reinterpret_cast<double *>(st + (size_t) a.cap_al * 8);
 				const int off = d.elem0 & 3;
+				const int4 pi = PK ? spack[s] : int4{};
+				const uint32_t * words = reinterpret_cast<const uint32_t *>(st + (size_t) a.cols_off);
 				// Rounds of WS_GATHER_SLOTS * ng consecutive entries, the same count for every gather
 				// thread; WS_GATHER_SLOTS independent loads in flight per thread.  The FMA formats'
 				// columns sit at the top of the x buffer: x of position p covers column positions
@@ -888,7 +921,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 					for (int k = 0; k < WS_GATHER_SLOTS; k++) {
 						const int e = e0 + k * ng;
 						if (e < d.elems)
-							xv[k] = ldg(a.x + sc[off + e]);
+							xv[k] = ldg(a.x + (PK ? packed_col64(words, e, pi.z, pi.y) : sc[off + e]));
 					}
 					if (A != Arith::SEQ_SPLIT)
 						named_bar_sync(2, ng);
@@ -924,7 +957,13 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 			if (b < b_end) {
 				const StagedBlock d = a.blocks[b];
 				sdesc[q] = d;
-				ws_issue(a, d, q, smem, full);
+				if (PK) {
+					const int4 pi = a.pinfo[b];
+					spack[q] = pi;
+					ws_issue_packed(a, d, pi, q, smem, full);
+				} else {
+					ws_issue(a, d, q, smem, full);
+				}
 			}
 		}
 	named_bar_sync(1, nr);
@@ -936,8 +975,12 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 	for (int64_t b = b_begin; b < b_end; b++) {
 		const int64_t nb = b + S;
 		StagedBlock dnext{};
-		if (rt == 0 && nb < b_end)
+		int4 pnext{};
+		if (rt == 0 && nb < b_end) {
 			dnext = a.blocks[nb];
+			if (PK)
+				pnext = a.pinfo[nb];
+		}
 		const StagedBlock d = sdesc[s];
 		int js0 = 0, je0 = 0;
 		int64_t yi = -1;
@@ -961,7 +1004,12 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		named_bar_sync(1, nr);
 		if (rt == 0 && nb < b_end) {
 			sdesc[s] = dnext;
-			ws_issue(a, dnext, s, smem, full);
+			if (PK) {
+				spack[s] = pnext;
+				ws_issue_packed(a, dnext, pnext, s, smem, full);
+			} else {
+				ws_issue(a, dnext, s, smem, full);
+			}
 		}
 		if (++s == S) {
 			s = 0;
@@ -1181,7 +1229,8 @@ StagedFn pick_ws(const Handle & h)
 {
 	const int fmt = h.desc.format;
 	if (fmt == SPMV_FMT_CSR_NAIVE)
-		return ws_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
+		return h.desc.pack_cols == 1 ? ws_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false, false, true>
+		                             : ws_kernel<Kind::CSR, Arith::SEQ_SPLIT, 1, false>;
 	if (fmt == SPMV_FMT_CSR_VEC) {
 		switch (h.desc.vec_len) {
 		case 1: return ws_kernel<Kind::CSR, Arith::LANES_FMA, 1, false>;
@@ -1548,6 +1597,8 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.stage_bytes = ws_stage_layout(fmt, a.cap_al, false, &a.cols_off);
 		a.row_threads = h.row_threads;
 		a.ranges = h.d_cta_ranges;
+		a.pinfo = h.d_pinfo;
+		a.pcols = h.d_pcols;
 	} else if (h.exec_kernel == 8) {
 		kern = pick_ws_tiled(h);
 		a.cols = h.d_tcols;

@@ -48,6 +48,19 @@ def test_csr_naive_fullsize(sb, orc, cfg):
     assert rel_row_error(y, gold, absy) <= TOL
 
 
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_csr_naive_packed_columns_fullsize(sb, orc, cfg):
+    """csr_naive with packed columns, FP64 and the FP32 variant: the same y bits as the
+    plain columns at both sizes."""
+    rp, ci, v, x = matrix(sb, cfg)
+    y = sb.csr_to_format(rp, ci, v, format="csr_naive", pack_cols=1).spmv(x)
+    assert np.array_equal(_bits(y), _bits(orc.csr_spmv(rp, ci, v, x)))
+    x32 = x.astype(np.float32)
+    y32p = sb.csr_to_format(rp, ci, v, format="csr_naive", value_type="f32", pack_cols=1).spmv(x32)
+    y32 = sb.csr_to_format(rp, ci, v, format="csr_naive", value_type="f32").spmv(x32)
+    assert np.array_equal(y32p.view(np.uint32), y32.view(np.uint32))
+
+
 @pytest.mark.parametrize("cfg,C,sigma", [("config1", 32, 256), ("config2", 32, 512)])
 def test_sellcs_fullsize(sb, orc, cfg, C, sigma):
     rp, ci, v, x = matrix(sb, cfg)

@@ -268,6 +268,34 @@ def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma):
             assert _eq_bits(y, ref).size == 0, (fmt, C, sigma, g["row_ptr"].size - 1)
 
 
+@pytest.mark.parametrize("block_nnz,stages", [(0, 0), (256, 3), (2048, 2)])
+def test_packed_columns_csr_naive(sb, orc, block_nnz, stages):
+    """pack_cols=1 on FP64 csr_naive (kernel 4 reads the columns packed per staged block):
+    the reference's y bits on every golden case, including long rows as chunk runs and
+    blocks whose columns span from 1 to 2^22 values."""
+    for name in golden_names():
+        g = load_golden(name)
+        mf = _mk(sb, g, "csr_naive", pack_cols=1, block_nnz=block_nnz, stages=stages)
+        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
+        assert _eq_bits(y, g["y_csr_naive"]).size == 0, (name, block_nnz)
+        assert np.array_equal(mf.export("col_ind"), g["col_ind"])
+    rng = np.random.default_rng(31)
+    m, n = 4000, 4000000
+    lens = rng.integers(0, 50, m)
+    lens[::211] = rng.integers(800, 6000, lens[::211].size)
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    spans = 2 ** rng.integers(0, 23, m)
+    ci = np.concatenate([np.sort(rng.integers(0, max(1, min(n, s)), k)) + rng.integers(0, n - min(n, s) + 1)
+                         for k, s in zip(lens, spans)]).astype(np.int32)
+    v = rng.uniform(-1, 1, ci.size)
+    x = rng.uniform(-1, 1, n)
+    mf = sb.csr_to_format(rp, ci, v, m, n, int(rp[-1]), format="csr_naive", pack_cols=1, block_nnz=block_nnz,
+                          stages=stages)
+    assert _eq_bits(mf.spmv(x, np.full(m, 1.0)), orc.csr_spmv(rp, ci, v, x)).size == 0
+    with pytest.raises(sb.SpmvError):
+        _mk(sb, load_golden("hand6"), "csr_vec", pack_cols=1)
+
+
 def test_tiled_kernel_rejects_small_blocks(sb):
     g = load_golden("hand6")
     with pytest.raises(sb.SpmvError):           # a block must hold one 8 x 32 tile
