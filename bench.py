@@ -278,7 +278,8 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     rp, ci, v, x = generate(sb, args)
     m, n, nnz = rp.size - 1, rp.size - 1, int(rp[-1])
-    B = algorithmic_bytes(m, n, nnz)
+    f32 = args.value_type == "f32"
+    B = algorithmic_bytes(m, n, nnz, 4, 4) if f32 else algorithmic_bytes(m, n, nnz)
     flops = 2.0 * nnz
     peak, peak_kind = hbm_peak()
 
@@ -291,8 +292,12 @@ def run_ours(args):
         except sb.SpmvError as e:
             per_format[fmt] = {"error": str(e)}
             continue
-        xd = torch.from_numpy(x).to(dev)
-        yd = torch.empty(m, dtype=torch.float64, device=dev)
+        if args.value_type == "f32" and fmt == args.format:
+            xd = torch.from_numpy(x.astype(np.float32)).to(dev)
+            yd = torch.empty(m, dtype=torch.float32, device=dev)
+        else:
+            xd = torch.from_numpy(x).to(dev)
+            yd = torch.empty(m, dtype=torch.float64, device=dev)
         sampler = ClockSampler(local) if fmt == args.format else None
         barrier(world)
         if sampler:
@@ -324,8 +329,8 @@ def run_ours(args):
 
     # e2e: public API with pinned host buffers; x H2D and y D2H inside every step
     mf = head["mf"]
-    xh = torch.from_numpy(x).pin_memory().numpy()
-    yh = torch.empty(m, dtype=torch.float64).pin_memory().numpy()
+    xh = torch.from_numpy(x.astype(np.float32) if f32 else x).pin_memory().numpy()
+    yh = torch.empty(m, dtype=torch.float32 if f32 else torch.float64).pin_memory().numpy()
     for _ in range(args.warmup):
         mf.spmv(xh, yh)
     barrier(world)
@@ -349,12 +354,12 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32" if f32 else "f64",
         "data": "synthetic (the reference's artificial generator restated natively, config 2; values 2v-1, x U[-1,1))",
         "config": make_config(args, args.format, m, n, nnz, B, world),
         "gflops": round(head["gflops"], 2),
-        "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s", "h2d_bytes_per_step": n * 8,
-                "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_s * 1e3, 4)},
+        "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s", "h2d_bytes_per_step": int(xh.nbytes),
+                "d2h_bytes_per_step": int(yh.nbytes), "ms_per_step": round(e2e_s * 1e3, 4)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
@@ -435,6 +440,17 @@ def tuned_legs(sb, torch, dev, rp, ci, v, x, per_format, B, peak, args):
         rec["tuned_tried"] = tried
 
 
+def mixed_classes(count):
+    """Batch formats dealt round robin over sell, sell_sorted, sell_c_s (C=32, sigma=512) and
+    csr_naive: a batch that runs the persistent work-queue kernel."""
+    from spmv_dare_b200 import tuning
+
+    pool = [tuning.CLASSES.index({"format": "sell", "vec_len": 4}),
+            tuning.CLASSES.index({"format": "sell_sorted", "vec_len": 4}),
+            tuning.CLASSES.index({"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 0}), 0]
+    return [pool[i % 4] for i in range(count)]
+
+
 def batch_block(sb, torch, dev, args, world, peak):
     """The 512-matrix batch (C4) inside the default line: the autotuned batch (every matrix
     csr_naive with these kernels: one block-diagonal SpMV, CUDA-graph replay) and the same
@@ -449,11 +465,7 @@ def batch_block(sb, torch, dev, args, world, peak):
     out = {"workload": BATCH_WORKLOAD, "matrices": len(mats), "bytes_per_step": B,
            "nnz_total": sum(int(mt[0][-1]) for mt in mats)}
     steps = max(5, args.steps // 2)
-    mixed_pool = [tuning.CLASSES.index({"format": "sell", "vec_len": 4}),
-                  tuning.CLASSES.index({"format": "sell_sorted", "vec_len": 4}),
-                  tuning.CLASSES.index({"format": "sell_c_s", "sellcs_c": 32, "sellcs_sigma": 512, "kernel": 0}),
-                  0]
-    legs = [("tuned", classes), ("mixed", [mixed_pool[i % 4] for i in range(len(mats))])]
+    legs = [("tuned", classes), ("mixed", mixed_classes(len(mats)))]
     for name, cls in legs:
         batch = sb.Batch(mats, [tuning.batch_desc(c) for c in cls])
         yd = torch.empty(batch.total_y, dtype=torch.float64, device=dev)
@@ -655,6 +667,8 @@ def run_batch(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     mats, classes, xs, B = batch_matrices(sb, args.batch_count, args.retune)
+    if args.batch_formats == "mixed":
+        classes = mixed_classes(len(mats))
     nnz_total = sum(int(mt[0][-1]) for mt in mats)
     batch = sb.Batch(mats, [tuning.batch_desc(c) for c in classes])
     xh = np.concatenate(xs)
@@ -836,11 +850,19 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="leave the batch block out of the default line")
     ap.add_argument("--no-tuned", action="store_true", help="time only the plain settings of each format")
     ap.add_argument("--params", default="", help="JSON object of descriptor fields for --format (profiling)")
+    ap.add_argument("--batch-formats", default="tuned", choices=["tuned", "mixed"],
+                    help="--workload batch: the autotuner's formats, or four formats dealt round robin")
+    ap.add_argument("--value-type", default="f64", choices=["f64", "f32"],
+                    help="headline line of csr_naive with FP32 values and FP32 vectors (the FP32 variant)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.params:
         FORMAT_PARAMS[args.format] = dict(FORMAT_PARAMS.get(args.format, {}), **json.loads(args.params))
+    if args.value_type == "f32":
+        if args.format != "csr_naive" or args.all_formats:
+            raise SystemExit("--value-type f32 times csr_naive alone (with --only-format)")
+        FORMAT_PARAMS["csr_naive"] = dict(FORMAT_PARAMS.get("csr_naive", {}), value_type="f32")
     if args.workload == "batch":
         (run_reference_batch if args.impl == "reference" else run_batch)(args)
     elif args.impl == "reference":
