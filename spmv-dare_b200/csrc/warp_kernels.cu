@@ -444,6 +444,63 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
+// Columns only, one tile ahead (the lighter form: a tile's values are requested beside its x,
+// so their DRAM latency overlaps the x gather; fewer registers, more warps an SM).
+__device__ __forceinline__ void tile_cols_load(const TileRegArgs & a, int64_t t0, int lane, int32_t (&c)[8])
+{
+	#pragma unroll
+	for (int q = 0; q < 8; q++)
+		c[q] = __ldcs(a.tcols + t0 + q * 32 + lane);
+}
+
+__device__ __forceinline__ void tile_reg_slice_light(const TileRegArgs & a, int64_t sl, int lane, int R)
+{
+	const int64_t b = a.sptr[sl];
+	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
+	const int nt = W >> 3, rem = W & 7;
+	double acc = 0.0;
+	int32_t c[8], cn[8];
+	if (nt > 0)
+		tile_cols_load(a, b, lane, c);
+	for (int t = 0; t < nt; t++) {
+		const int64_t t0 = b + (int64_t) t * 256;
+		double X[8], v[8];
+		#pragma unroll
+		for (int q = 0; q < 8; q++)
+			X[q] = __ldg(a.x + c[q]);
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			v[j] = __ldcs(a.vals + t0 + j * 32 + R);
+		if (t + 1 < nt)
+			tile_cols_load(a, t0 + 256, lane, cn);
+		transpose8(X, lane);
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			acc = __fma_rn(v[j], X[j], acc);
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			c[j] = cn[j];
+	}
+	if (rem > 0) {
+		const int64_t t0 = b + (int64_t) nt * 256;
+		double X[8], vv[8];
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			if (j < rem) {
+				X[j] = __ldg(a.x + __ldcs(a.tcols + t0 + R * rem + j));
+				vv[j] = __ldcs(a.vals + t0 + j * 32 + R);
+			}
+		}
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			if (j < rem)
+				acc = __fma_rn(vv[j], X[j], acc);
+	}
+	const int64_t row = sl * 32 + R;
+	if (row < a.m)
+		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
+}
+
 __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int lane, int R)
 {
 	const int64_t b = a.sptr[sl];
@@ -491,7 +548,10 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
 }
 
-__global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
+// LIGHT: the columns-only prefetch (3 CTAs an SM); otherwise columns and values one tile
+// ahead (2 CTAs an SM).
+template <bool LIGHT>
+__global__ void __launch_bounds__(TILE_REG_THREADS, LIGHT ? 3 : 2) tile_reg_kernel(TileRegArgs a)
 {
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
@@ -503,8 +563,12 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 		if ((int64_t) it >= a.nitems)
 			break;
 		const int2 r = a.items[it];
-		for (int64_t sl = r.x; sl < r.y; sl++)
-			tile_reg_slice(a, sl, lane, R);
+		for (int64_t sl = r.x; sl < r.y; sl++) {
+			if (LIGHT)
+				tile_reg_slice_light(a, sl, lane, R);
+			else
+				tile_reg_slice(a, sl, lane, R);
+		}
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
 	// finish puts the queue back to zero for the next launch
@@ -761,6 +825,8 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 		set_error(SPMV_ERR_ARG, "kernel 10 takes slices of exactly 32 rows (got %d)", V);
 		return SPMV_ERR_ARG;
 	}
+	// stages = 1: the lighter form (columns prefetched, values beside the x loads); else both
+	h.stages = h.desc.stages == 1 ? 1 : 2;
 	cudaStream_t s = h.stream;
 	std::vector<int32_t> P((size_t) U + 1);
 	SPMV_CUDA_TRY(cudaMemcpyAsync(P.data(), d_P, (U + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -791,7 +857,8 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+				h.stages == 1 ? tile_reg_kernel<true> : tile_reg_kernel<false>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -825,7 +892,10 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		tile_reg_kernel<<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		if (h.stages == 1)
+			tile_reg_kernel<true><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else
+			tile_reg_kernel<false><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}
