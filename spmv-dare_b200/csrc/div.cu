@@ -615,6 +615,7 @@ __device__ __forceinline__ uint32_t ld_u32(const uint8_t * p)
 
 struct DivArgs {
 	const uint8_t * data;
+	int64_t data_bytes;          // bytes of the packet stream
 	const int64_t * pkt_off;
 	const int4 * meta;
 	int64_t npackets;
@@ -801,10 +802,12 @@ constexpr int DIVW_WARPS = 8;
 
 struct LaneReader {
 	const uint64_t * w;      // next aligned word to load
+	const uint64_t * lim;    // prefetches stay below this word (the end of the packet data)
 	uint64_t cur, nxt;       // the words holding the read position and the one after it
 	int sh;                  // read position within cur, in bytes
-	__device__ __forceinline__ void init(const uint8_t * p)
+	__device__ __forceinline__ void init(const uint8_t * p, const uint8_t * end)
 	{
+		lim = reinterpret_cast<const uint64_t *>(reinterpret_cast<uintptr_t>(end) & ~(uintptr_t) 7);
 		const uintptr_t a = reinterpret_cast<uintptr_t>(p);
 		w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t) 7);
 		sh = (int) (a & 7);
@@ -812,7 +815,9 @@ struct LaneReader {
 		nxt = w[1];
 		w += 2;
 	}
-	// n <= 8 little-endian bytes; reads reach at most 15 bytes past the read position
+	// n <= 8 little-endian bytes; reads reach at most 15 bytes past the read position.  On
+	// entering a new 128-byte line the line two ahead is requested (an L1 prefetch hint: a
+	// lane's stream is read in order, and its first touch of a line would stall the chain)
 	__device__ __forceinline__ uint64_t read(int n)
 	{
 		const uint64_t v = sh ? ((cur >> (8 * sh)) | (nxt << (64 - 8 * sh))) : cur;
@@ -820,6 +825,8 @@ struct LaneReader {
 		if (sh >= 8) {
 			sh -= 8;
 			cur = nxt;
+			if ((reinterpret_cast<uintptr_t>(w) & 127) == 0 && w + 32 < lim)
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(w + 32));
 			nxt = *w++;
 		}
 		return n >= 8 ? v : (v & ((1ULL << (8 * n)) - 1));
@@ -861,7 +868,7 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 	}
 	start -= my_bytes;
 	LaneReader rd;
-	rd.init(lanes + start);
+	rd.init(lanes + start, a.data + a.data_bytes);
 	__syncwarp();
 	int kstart = 0, cstart = 0;
 	for (int g = 0; g < nrf; g++) {
@@ -1427,6 +1434,7 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	}
 	DivArgs a;
 	a.data = h.d_div;
+	a.data_bytes = h.div_bytes;
 	a.pkt_off = h.d_pkt;
 	a.meta = h.d_pkt_meta;
 	a.npackets = h.num_packets;
