@@ -75,17 +75,21 @@ def evaluate(sel, db):
 def mlp_cost(sb, sel, db, count=8):
     """Seconds per matrix of the MLP's tuning: device features + one forward pass (host
     wall time, median of 3 queries per matrix, median over `count` held-out matrices
-    regenerated from their seeds; the CSR arrays are already on the GPU)."""
+    regenerated on the GPU from their stored parameters; the CSR arrays are already on the
+    GPU)."""
     import torch
 
     from spmv_dare_b200 import selector, workloads
 
     costs = []
-    for seed in db["seeds"][:count].tolist():
-        p = workloads.selector_params(int(seed))
-        rp, ci, _, _ = workloads.generate(sb, p)
-        m, n, nnz = rp.size - 1, p["cols"], int(rp[-1])
-        drp, dci = torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda()
+    names = [str(k) for k in db["param_names"]]
+    for i in range(min(count, db["seeds"].size)):
+        q = dict(zip(names, db["params"][i].tolist()))
+        p = dict(rows=int(q["rows"]), cols=int(q["rows"]), avg=q["avg"], std=q["std"], skew=q["skew"], bw=q["bw"],
+                 neigh=q["neigh"], cross=q["cross"], distribution="gamma" if db["gamma"][i] else "normal",
+                 placement="random", seed=int(db["seeds"][i]))
+        drp, dci, _ = workloads.generate_device(sb, p)
+        m, n, nnz = p["rows"], p["cols"], int(dci.numel())
         sel.predict(selector.features_device(drp, dci, m, n, nnz))          # warm-up
         torch.cuda.synchronize()
         per = []
