@@ -799,6 +799,7 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 // bytes consumed), the coordinates (neighbouring for rf = 1) and x; products go to the
 // warp's row sums in shared memory, then the packet's rows are stored as in the CTA decoder.
 constexpr int DIVW_WARPS = 8;
+constexpr int DIVW_BATCH = 4;    // positions a lane decodes per step of the rf = 1 loop
 
 struct LaneReader {
 	const uint64_t * w;      // next aligned word to load
@@ -833,7 +834,7 @@ struct LaneReader {
 	}
 };
 
-__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
+__global__ void __launch_bounds__(DIVW_WARPS * 32, 3) div_warp_kernel(DivArgs a)
 {
 	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -877,26 +878,46 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 		const int n_i = dv + (lane < md ? 1 : 0);
 		uint64_t val = 0;                                   // differences restart in every group
 		if (rf == 1) {
-			for (int pos0 = 0; pos0 < n_i; pos0 += 4) {
-				double vv[4], xv[4];
-				int rr[4];
+			// batches of DIVW_BATCH positions; the next batch's code bytes and coordinates are
+			// requested before this batch is decoded, so only the x gather is on the chain
+			uint32_t cd[DIVW_BATCH];
+			uint64_t cc[DIVW_BATCH];
+			#pragma unroll
+			for (int q = 0; q < DIVW_BATCH; q++) {
+				const int k = q * 32 + lane;
+				cd[q] = q < n_i ? codes[kstart + k] : 0u;
+				cc[q] = q < n_i ? ld_bytes(coords + (int64_t) (cstart + k) * cb, cb) : 0;
+			}
+			for (int pos0 = 0; pos0 < n_i; pos0 += DIVW_BATCH) {
+				uint32_t cdn[DIVW_BATCH];
+				uint64_t ccn[DIVW_BATCH];
 				#pragma unroll
-				for (int q = 0; q < 4; q++) {
-					const int pos = pos0 + q;
-					if (pos < n_i) {
-						const int k = pos * 32 + lane;
-						const uint8_t code = codes[kstart + k];
-						val += rd.read(code & 15) << ((code >> 4) << 2);
+				for (int q = 0; q < DIVW_BATCH; q++) {
+					const int pos = pos0 + DIVW_BATCH + q;
+					const int k = pos * 32 + lane;
+					cdn[q] = pos < n_i ? codes[kstart + k] : 0u;
+					ccn[q] = pos < n_i ? ld_bytes(coords + (int64_t) (cstart + k) * cb, cb) : 0;
+				}
+				double vv[DIVW_BATCH], xv[DIVW_BATCH];
+				int rr[DIVW_BATCH];
+				#pragma unroll
+				for (int q = 0; q < DIVW_BATCH; q++) {
+					if (pos0 + q < n_i) {
+						val += rd.read((int) (cd[q] & 15)) << ((cd[q] >> 4) << 2);
 						vv[q] = __longlong_as_double((long long) val);
-						const uint64_t c = ld_bytes(coords + (int64_t) (cstart + k) * cb, cb);
-						rr[q] = (int) (c & rmask);
-						xv[q] = __ldg(a.x + col_min + (int64_t) ((c >> row_bits) & cmask));
+						rr[q] = (int) (cc[q] & rmask);
+						xv[q] = __ldg(a.x + col_min + (int64_t) ((cc[q] >> row_bits) & cmask));
 					}
 				}
 				#pragma unroll
-				for (int q = 0; q < 4; q++)
+				for (int q = 0; q < DIVW_BATCH; q++)
 					if (pos0 + q < n_i)
 						atomicAdd(&ys[rr[q]], vv[q] * xv[q]);
+				#pragma unroll
+				for (int q = 0; q < DIVW_BATCH; q++) {
+					cd[q] = cdn[q];
+					cc[q] = ccn[q];
+				}
 			}
 		} else {
 			for (int pos = 0; pos < n_i; pos++) {
