@@ -157,6 +157,8 @@ typedef struct spmv_info {
 	char    format_name[64];     /* the reference's format_name, e.g. "Naive_CSR_CPU" -> "Naive_CSR_GPU" */
 	double  alloc_ms;            /* part of convert_ms spent in cudaMalloc                         */
 	double  copy_in_ms;          /* part of convert_ms spent copying the CSR arrays to the device  */
+	int64_t x_lo, x_hi;          /* span of x the converted format reads (its stored columns, padding
+	                                included); spmv_run / spmv_run_f32 copy only x[x_lo..x_hi] */
 } spmv_info;
 
 /* Fill *desc with the defaults above for `format`. */
@@ -177,7 +179,8 @@ spmv_handle * spmv_create(const int32_t * row_ptr, const int32_t * col_ind, cons
 spmv_handle * spmv_create_device(const int32_t * d_row_ptr, const int32_t * d_col_ind, const double * d_values,
 		int64_t m, int64_t n, int64_t nnz, const spmv_format_desc * desc, void * stream, int * status);
 
-/* Matrix_Format::spmv(x, y) with HOST buffers: x[n] -> device, y[m] <- device, synchronous.
+/* Matrix_Format::spmv(x, y) with HOST buffers: x -> device (only x[x_lo..x_hi], the span the
+ * converted matrix reads, see spmv_info), y[m] <- device, synchronous.
  * Rows without entries get 0 (the reference's y=1.0 probe, bench_spmv.cpp:561-564). */
 int spmv_run(spmv_handle * h, const double * x, double * y);
 

@@ -123,6 +123,7 @@ class Matrix_Format:
         self.convert_ms = float(info.convert_ms)
         self.alloc_ms = float(info.alloc_ms)
         self.copy_in_ms = float(info.copy_in_ms)
+        self.x_span = (int(info.x_lo), int(info.x_hi))    # the part of x the matrix reads
         self.kernels_per_run = int(info.kernels_per_run)
         self.num_loops = 0
 

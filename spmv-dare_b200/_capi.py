@@ -64,6 +64,7 @@ class Info(ctypes.Structure):
         ("csr_mem_footprint", c_double), ("stored_elems", c_int64), ("device_bytes", c_int64),
         ("convert_ms", c_double), ("kernels_per_run", c_int32), ("format", c_int32),
         ("format_name", c_char * 64), ("alloc_ms", c_double), ("copy_in_ms", c_double),
+        ("x_lo", c_int64), ("x_hi", c_int64),
     ]
 
 

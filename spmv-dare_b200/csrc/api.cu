@@ -178,6 +178,59 @@ static int init_device(Handle & h)
 	return SPMV_OK;
 }
 
+// Smallest and largest column index of a stored column array (padding included).
+__global__ void col_span_kernel(const int32_t * c, int64_t n, int * lo_hi)
+{
+	int lo = INT32_MAX, hi = -1;
+	for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+		lo = min(lo, c[i]);
+		hi = max(hi, c[i]);
+	}
+	#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+		hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicMin(&lo_hi[0], lo);
+		atomicMax(&lo_hi[1], hi);
+	}
+}
+
+// The span of x the converted format reads: the stored column array of the format (SELL's
+// and SELL-C-sigma's padding columns included; DIV-RF reads the CSR columns).  spmv_run
+// copies only that part of a host x to the device.
+static int set_x_span(Handle & h)
+{
+	const int32_t * c = h.d_ci;
+	int64_t cnt = h.nnz;
+	if (h.desc.format == SPMV_FMT_SELL || h.desc.format == SPMV_FMT_SELL_SORTED) {
+		c = h.d_ja;
+		cnt = h.nnz_ext;
+	} else if (h.desc.format == SPMV_FMT_SELL_C_S) {
+		c = h.d_scols;
+		cnt = h.sellcs_size;
+	}
+	h.x_lo = 0;
+	h.x_hi = -1;
+	if (cnt <= 0 || h.n <= 0)
+		return SPMV_OK;
+	int * d = nullptr;
+	SPMV_TRY(h.alloc(&d, 2));
+	const int init[2] = {INT32_MAX, -1};
+	SPMV_CUDA_TRY(cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, h.stream));
+	col_span_kernel<<<(unsigned) (cnt < 256 * 148 * 4 ? ceil_div(cnt, 256) : 148 * 4), 256, 0, h.stream>>>(c, cnt, d);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	int lh[2];
+	SPMV_CUDA_TRY(cudaMemcpyAsync(lh, d, sizeof(lh), cudaMemcpyDeviceToHost, h.stream));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(h.stream));
+	if (lh[1] >= 0) {
+		h.x_lo = lh[0];
+		h.x_hi = lh[1];
+	}
+	return SPMV_OK;
+}
+
 static int convert_all(Handle & h)
 {
 	SPMV_TRY(validate_csr(h));
@@ -206,6 +259,7 @@ static int convert_all(Handle & h)
 	}
 	SPMV_CUDA_TRY(cudaStreamSynchronize(h.stream));
 	set_footprints(h);
+	SPMV_TRY(set_x_span(h));
 	h.name = kNames[h.desc.format];
 	if (h.desc.values == SPMV_VALUES_F32)
 		h.name = "Naive_CSR_F32_Dot2_B200";
@@ -412,8 +466,9 @@ int spmv_run(spmv_handle * H, const double * x, double * y)
 		SPMV_TRY(h.alloc(&h.d_y, h.m + 1));
 	}
 	cudaStream_t s = h.stream;
-	if (h.n > 0)
-		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_x, x, h.n * sizeof(double), cudaMemcpyHostToDevice, s));
+	if (h.x_hi >= h.x_lo)           // only the span of x the matrix reads
+		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_x + h.x_lo, x + h.x_lo, (h.x_hi - h.x_lo + 1) * sizeof(double),
+				cudaMemcpyHostToDevice, s));
 	if (h.desc.values == SPMV_VALUES_F32) {
 		// FP32 handle driven with FP64 buffers: round x once, widen y
 		if (!h.d_xf) {
@@ -449,7 +504,9 @@ int spmv_run_f32(spmv_handle * H, const float * x, float * y)
 	}
 	cudaStream_t s = h.stream;
 	if (h.n > 0)
-		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_xf, x, h.n * sizeof(float), cudaMemcpyHostToDevice, s));
+		if (h.x_hi >= h.x_lo)
+			SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_xf + h.x_lo, x + h.x_lo, (h.x_hi - h.x_lo + 1) * sizeof(float),
+					cudaMemcpyHostToDevice, s));
 	SPMV_TRY(spmv::launch_spmv_f32(h, h.d_xf, h.d_yf, s));
 	if (h.m > 0)
 		SPMV_CUDA_TRY(cudaMemcpyAsync(y, h.d_yf, h.m * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -496,6 +553,8 @@ int spmv_get_info(const spmv_handle * H, spmv_info * out)
 	out->convert_ms = h.convert_ms;
 	out->alloc_ms = h.alloc_ms;
 	out->copy_in_ms = h.copy_in_ms;
+	out->x_lo = h.x_lo;
+	out->x_hi = h.x_hi;
 	out->kernels_per_run = h.kernels_per_run;
 	out->format = h.desc.format;
 	snprintf(out->format_name, sizeof(out->format_name), "%s", h.name.c_str());
