@@ -60,9 +60,7 @@ TUNED = {
     "csr_vec": [dict(vec_len=8), dict(vec_len=2)],
     "sell": [dict(vec_len=8), dict(vec_len=16), dict(vec_len=32, kernel=10), dict(vec_len=32, kernel=8)],
     "sell_sorted": [dict(vec_len=8), dict(vec_len=32, kernel=10), dict(vec_len=32, kernel=8)],
-    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, kernel=10), dict(sellcs_c=32, sellcs_sigma=512, kernel=10, stages=1),
-                 dict(sellcs_c=32, sellcs_sigma=512, kernel=10, stages=3),
-                 dict(sellcs_c=32, sellcs_sigma=4096, kernel=10),
+    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, kernel=10), dict(sellcs_c=32, sellcs_sigma=4096, kernel=10),
                  dict(sellcs_c=32, sellcs_sigma=32, kernel=10), dict(sellcs_c=64, sellcs_sigma=1024, kernel=8)],
     "div_rf": [dict(vec_len=32), dict(vec_len=32, div_packet_vals=4096), dict(vec_len=32, div_packet_vals=65536)],
 }

@@ -615,7 +615,6 @@ __device__ __forceinline__ uint32_t ld_u32(const uint8_t * p)
 
 struct DivArgs {
 	const uint8_t * data;
-	int64_t data_bytes;          // bytes of the packet stream
 	const int64_t * pkt_off;
 	const int4 * meta;
 	int64_t npackets;
@@ -799,16 +798,13 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 // bytes consumed), the coordinates (neighbouring for rf = 1) and x; products go to the
 // warp's row sums in shared memory, then the packet's rows are stored as in the CTA decoder.
 constexpr int DIVW_WARPS = 8;
-constexpr int DIVW_BATCH = 4;    // positions a lane decodes per step of the rf = 1 loop
 
 struct LaneReader {
 	const uint64_t * w;      // next aligned word to load
-	const uint64_t * lim;    // prefetches stay below this word (the end of the packet data)
 	uint64_t cur, nxt;       // the words holding the read position and the one after it
 	int sh;                  // read position within cur, in bytes
-	__device__ __forceinline__ void init(const uint8_t * p, const uint8_t * end)
+	__device__ __forceinline__ void init(const uint8_t * p)
 	{
-		lim = reinterpret_cast<const uint64_t *>(reinterpret_cast<uintptr_t>(end) & ~(uintptr_t) 7);
 		const uintptr_t a = reinterpret_cast<uintptr_t>(p);
 		w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t) 7);
 		sh = (int) (a & 7);
@@ -816,9 +812,7 @@ struct LaneReader {
 		nxt = w[1];
 		w += 2;
 	}
-	// n <= 8 little-endian bytes; reads reach at most 15 bytes past the read position.  On
-	// entering a new 128-byte line the line two ahead is requested (an L1 prefetch hint: a
-	// lane's stream is read in order, and its first touch of a line would stall the chain)
+	// n <= 8 little-endian bytes; reads reach at most 15 bytes past the read position
 	__device__ __forceinline__ uint64_t read(int n)
 	{
 		const uint64_t v = sh ? ((cur >> (8 * sh)) | (nxt << (64 - 8 * sh))) : cur;
@@ -826,15 +820,13 @@ struct LaneReader {
 		if (sh >= 8) {
 			sh -= 8;
 			cur = nxt;
-			if ((reinterpret_cast<uintptr_t>(w) & 127) == 0 && w + 32 < lim)
-				asm volatile("prefetch.global.L1 [%0];" ::"l"(w + 32));
 			nxt = *w++;
 		}
 		return n >= 8 ? v : (v & ((1ULL << (8 * n)) - 1));
 	}
 };
 
-__global__ void __launch_bounds__(DIVW_WARPS * 32, 3) div_warp_kernel(DivArgs a)
+__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 {
 	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -869,7 +861,7 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32, 3) div_warp_kernel(DivArgs a)
 	}
 	start -= my_bytes;
 	LaneReader rd;
-	rd.init(lanes + start, a.data + a.data_bytes);
+	rd.init(lanes + start);
 	__syncwarp();
 	int kstart = 0, cstart = 0;
 	for (int g = 0; g < nrf; g++) {
@@ -878,46 +870,26 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32, 3) div_warp_kernel(DivArgs a)
 		const int n_i = dv + (lane < md ? 1 : 0);
 		uint64_t val = 0;                                   // differences restart in every group
 		if (rf == 1) {
-			// batches of DIVW_BATCH positions; the next batch's code bytes and coordinates are
-			// requested before this batch is decoded, so only the x gather is on the chain
-			uint32_t cd[DIVW_BATCH];
-			uint64_t cc[DIVW_BATCH];
-			#pragma unroll
-			for (int q = 0; q < DIVW_BATCH; q++) {
-				const int k = q * 32 + lane;
-				cd[q] = q < n_i ? codes[kstart + k] : 0u;
-				cc[q] = q < n_i ? ld_bytes(coords + (int64_t) (cstart + k) * cb, cb) : 0;
-			}
-			for (int pos0 = 0; pos0 < n_i; pos0 += DIVW_BATCH) {
-				uint32_t cdn[DIVW_BATCH];
-				uint64_t ccn[DIVW_BATCH];
+			for (int pos0 = 0; pos0 < n_i; pos0 += 4) {
+				double vv[4], xv[4];
+				int rr[4];
 				#pragma unroll
-				for (int q = 0; q < DIVW_BATCH; q++) {
-					const int pos = pos0 + DIVW_BATCH + q;
-					const int k = pos * 32 + lane;
-					cdn[q] = pos < n_i ? codes[kstart + k] : 0u;
-					ccn[q] = pos < n_i ? ld_bytes(coords + (int64_t) (cstart + k) * cb, cb) : 0;
-				}
-				double vv[DIVW_BATCH], xv[DIVW_BATCH];
-				int rr[DIVW_BATCH];
-				#pragma unroll
-				for (int q = 0; q < DIVW_BATCH; q++) {
-					if (pos0 + q < n_i) {
-						val += rd.read((int) (cd[q] & 15)) << ((cd[q] >> 4) << 2);
+				for (int q = 0; q < 4; q++) {
+					const int pos = pos0 + q;
+					if (pos < n_i) {
+						const int k = pos * 32 + lane;
+						const uint8_t code = codes[kstart + k];
+						val += rd.read(code & 15) << ((code >> 4) << 2);
 						vv[q] = __longlong_as_double((long long) val);
-						rr[q] = (int) (cc[q] & rmask);
-						xv[q] = __ldg(a.x + col_min + (int64_t) ((cc[q] >> row_bits) & cmask));
+						const uint64_t c = ld_bytes(coords + (int64_t) (cstart + k) * cb, cb);
+						rr[q] = (int) (c & rmask);
+						xv[q] = __ldg(a.x + col_min + (int64_t) ((c >> row_bits) & cmask));
 					}
 				}
 				#pragma unroll
-				for (int q = 0; q < DIVW_BATCH; q++)
+				for (int q = 0; q < 4; q++)
 					if (pos0 + q < n_i)
 						atomicAdd(&ys[rr[q]], vv[q] * xv[q]);
-				#pragma unroll
-				for (int q = 0; q < DIVW_BATCH; q++) {
-					cd[q] = cdn[q];
-					cc[q] = ccn[q];
-				}
 			}
 		} else {
 			for (int pos = 0; pos < n_i; pos++) {
@@ -1455,7 +1427,6 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	}
 	DivArgs a;
 	a.data = h.d_div;
-	a.data_bytes = h.div_bytes;
 	a.pkt_off = h.d_pkt;
 	a.meta = h.d_pkt_meta;
 	a.npackets = h.num_packets;

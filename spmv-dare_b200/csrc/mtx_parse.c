@@ -18,7 +18,9 @@
  *     number that sets errno (out of range, a subnormal value) is an error there and here;
  *   - with symmetry and expand_symmetry, the mirror (col, row) of every off-diagonal entry
  *     is appended after all stored entries, in their order, its value negated for
- *     skew-symmetric files (matrix_market_gen.c:62-127);
+ *     skew-symmetric files (matrix_market_gen.c:62-127), in the type the field is read
+ *     into: a real 0 becomes -0.0, an integer 0 stays 0 (integers are read as int,
+ *     matrix_market.c:23-27, 288-293);
  *   - values become real: integer -> double, complex -> cabs(value) (the conjugate of a
  *     Hermitian mirror has the same modulus), pattern -> 1.0.
  */
@@ -232,8 +234,14 @@ int mtx_parse_file(const char * path, int expand_symmetry, struct mtx_coo * out)
 			if (out->R[k] != out->C[k]) {
 				out->R[j] = out->C[k];
 				out->C[j] = out->R[k];
-				/* a complex value is already its modulus: |-conj(z)| = |z| */
-				out->V[j] = (skew && field != 2) ? -out->V[k] : out->V[k];
+				/* a complex value is already its modulus: |-conj(z)| = |z|; an integer value
+				 * is negated as the int it was read into (0 stays +0.0, INT_MIN wraps) */
+				if (!skew || field == 2)
+					out->V[j] = out->V[k];
+				else if (field == 1)
+					out->V[j] = (double) (int32_t) (0u - (uint32_t) (int32_t) out->V[k]);
+				else
+					out->V[j] = -out->V[k];
 				j++;
 			}
 		}

@@ -444,63 +444,6 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
-// Columns only, one tile ahead (the lighter form: a tile's values are requested beside its x,
-// so their DRAM latency overlaps the x gather; fewer registers, more warps an SM).
-__device__ __forceinline__ void tile_cols_load(const TileRegArgs & a, int64_t t0, int lane, int32_t (&c)[8])
-{
-	#pragma unroll
-	for (int q = 0; q < 8; q++)
-		c[q] = __ldcs(a.tcols + t0 + q * 32 + lane);
-}
-
-__device__ __forceinline__ void tile_reg_slice_light(const TileRegArgs & a, int64_t sl, int lane, int R)
-{
-	const int64_t b = a.sptr[sl];
-	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
-	const int nt = W >> 3, rem = W & 7;
-	double acc = 0.0;
-	int32_t c[8], cn[8];
-	if (nt > 0)
-		tile_cols_load(a, b, lane, c);
-	for (int t = 0; t < nt; t++) {
-		const int64_t t0 = b + (int64_t) t * 256;
-		double X[8], v[8];
-		#pragma unroll
-		for (int q = 0; q < 8; q++)
-			X[q] = __ldg(a.x + c[q]);
-		#pragma unroll
-		for (int j = 0; j < 8; j++)
-			v[j] = __ldcs(a.vals + t0 + j * 32 + R);
-		if (t + 1 < nt)
-			tile_cols_load(a, t0 + 256, lane, cn);
-		transpose8(X, lane);
-		#pragma unroll
-		for (int j = 0; j < 8; j++)
-			acc = __fma_rn(v[j], X[j], acc);
-		#pragma unroll
-		for (int j = 0; j < 8; j++)
-			c[j] = cn[j];
-	}
-	if (rem > 0) {
-		const int64_t t0 = b + (int64_t) nt * 256;
-		double X[8], vv[8];
-		#pragma unroll
-		for (int j = 0; j < 8; j++) {
-			if (j < rem) {
-				X[j] = __ldg(a.x + __ldcs(a.tcols + t0 + R * rem + j));
-				vv[j] = __ldcs(a.vals + t0 + j * 32 + R);
-			}
-		}
-		#pragma unroll
-		for (int j = 0; j < 8; j++)
-			if (j < rem)
-				acc = __fma_rn(vv[j], X[j], acc);
-	}
-	const int64_t row = sl * 32 + R;
-	if (row < a.m)
-		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
-}
-
 __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int lane, int R)
 {
 	const int64_t b = a.sptr[sl];
@@ -548,82 +491,8 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
 }
 
-// A tile of width w (8: a full tile in the row-major 8-column order; below 8: a slice's
-// narrower last tile, rows at R * w) from entry t0: lane L's 8 column indices and its row's
-// values.  Full tiles: index q is tile entry q * 32 + L (transposed after the x loads);
-// narrower ones: index j is column j of row R (no transpose).
-__device__ __forceinline__ void any_tile_load(const TileRegArgs & a, int64_t t0, int w, int lane, int R,
-		int32_t (&c)[8], double (&v)[8])
+__global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
 {
-	if (w == 8) {
-		tile_load(a, t0, lane, R, c, v);
-		return;
-	}
-	#pragma unroll
-	for (int j = 0; j < 8; j++) {
-		c[j] = j < w ? __ldcs(a.tcols + t0 + R * w + j) : 0;
-		v[j] = j < w ? __ldcs(a.vals + t0 + j * 32 + R) : 0.0;
-	}
-}
-
-// One work item (slices s0 .. s0 + ns - 1, ns <= 31) with the next tile always in flight,
-// across slice boundaries too: lane k holds slice pointer s0 + k, so a slice's first tile is
-// requested while the previous slice's last tile is summed.
-__device__ __forceinline__ void tile_reg_item(const TileRegArgs & a, int64_t s0, int ns, int lane, int R)
-{
-	const int32_t myp = lane <= ns ? a.sptr[s0 + lane] : 0;
-	int32_t c[8], cn[8];
-	double v[8], vn[8];
-	bool have = false;                 // (c, v) already hold the slice's first tile
-	for (int k = 0; k < ns; k++) {
-		const int64_t b = __shfl_sync(0xffffffffu, myp, k);
-		const int W = (int) (((int64_t) __shfl_sync(0xffffffffu, myp, k + 1) - b) >> 5);
-		const int nt = W >> 3, rem = W & 7, T = nt + (rem > 0);
-		// the next slice's first tile: its base is this slice's end
-		int wn = 0;
-		if (k + 1 < ns) {
-			const int Wn = (int) (((int64_t) __shfl_sync(0xffffffffu, myp, k + 2) - b) >> 5) - W;
-			wn = Wn >= 8 ? 8 : Wn;
-		}
-		if (T > 0 && !have)
-			any_tile_load(a, b, nt > 0 ? 8 : rem, lane, R, c, v);
-		double acc = 0.0;
-		for (int t = 0; t < T; t++) {
-			const int w = t < nt ? 8 : rem;
-			if (t + 1 < T)
-				any_tile_load(a, b + (int64_t) (t + 1) * 256, t + 1 < nt ? 8 : rem, lane, R, cn, vn);
-			else if (wn > 0)
-				any_tile_load(a, b + (int64_t) W * 32, wn, lane, R, cn, vn);
-			double X[8];
-			#pragma unroll
-			for (int q = 0; q < 8; q++)
-				X[q] = q < w ? __ldg(a.x + c[q]) : 0.0;
-			if (w == 8)
-				transpose8(X, lane);
-			#pragma unroll
-			for (int j = 0; j < 8; j++)
-				if (j < w)
-					acc = __fma_rn(v[j], X[j], acc);
-			#pragma unroll
-			for (int j = 0; j < 8; j++) {
-				c[j] = cn[j];
-				v[j] = vn[j];
-			}
-		}
-		have = T > 0 && wn > 0;
-		const int64_t row = (s0 + k) * 32 + R;
-		if (row < a.m)
-			a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
-	}
-}
-
-// FORM 1: the columns-only prefetch (80 registers, 3 CTAs an SM); FORM 2: columns and values
-// one tile ahead, across slice boundaries (100 registers, 2 CTAs an SM); FORM 3: FORM 2 held
-// to 3 CTAs an SM (80 registers, a few spilled).
-template <int FORM>
-__global__ void __launch_bounds__(TILE_REG_THREADS, FORM == 2 ? 2 : 3) tile_reg_kernel(TileRegArgs a)
-{
-	constexpr bool LIGHT = FORM == 1;
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
 	for (;;) {
@@ -634,12 +503,8 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, FORM == 2 ? 2 : 3) tile_reg_
 		if ((int64_t) it >= a.nitems)
 			break;
 		const int2 r = a.items[it];
-		if (LIGHT) {
-			for (int64_t sl = r.x; sl < r.y; sl++)
-				tile_reg_slice_light(a, sl, lane, R);
-		} else {
-			tile_reg_item(a, r.x, r.y - r.x, lane, R);
-		}
+		for (int64_t sl = r.x; sl < r.y; sl++)
+			tile_reg_slice(a, sl, lane, R);
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
 	// finish puts the queue back to zero for the next launch
@@ -887,8 +752,7 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 
 // Work items of kernel 10: slices of at least TILE_REG_HEAVY entries alone, the heaviest
 // first; the others in matrix order, in runs of consecutive slices of about
-// TILE_REG_ITEM entries and at most 31 slices (neighbouring rows keep x warm in L2; a warp
-// holds an item's slice pointers one per lane).
+// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2).
 constexpr int64_t TILE_REG_HEAVY = 4096, TILE_REG_ITEM = 2048;
 
 int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
@@ -897,9 +761,6 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 		set_error(SPMV_ERR_ARG, "kernel 10 takes slices of exactly 32 rows (got %d)", V);
 		return SPMV_ERR_ARG;
 	}
-	// stages = 1: the lighter form (columns prefetched, values beside the x loads); 3: the
-	// cross-slice pipeline at 3 CTAs an SM; otherwise the cross-slice pipeline at 2
-	h.stages = (h.desc.stages == 1 || h.desc.stages == 3) ? h.desc.stages : 2;
 	cudaStream_t s = h.stream;
 	std::vector<int32_t> P((size_t) U + 1);
 	SPMV_CUDA_TRY(cudaMemcpyAsync(P.data(), d_P, (U + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -914,7 +775,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 			continue;
 		}
 		const int64_t u0 = u, e0 = P[u];
-		while (u < U && u - u0 < 31 && (int64_t) P[u + 1] - P[u] < TILE_REG_HEAVY && (int64_t) P[u] - e0 < TILE_REG_ITEM)
+		while (u < U && (int64_t) P[u + 1] - P[u] < TILE_REG_HEAVY && (int64_t) P[u] - e0 < TILE_REG_ITEM)
 			u++;
 		rest.push_back(make_int2((int) u0, (int) u));
 	}
@@ -930,9 +791,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-				h.stages == 1 ? tile_reg_kernel<1> : h.stages == 3 ? tile_reg_kernel<3> : tile_reg_kernel<2>,
-				TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -966,12 +825,7 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		if (h.stages == 1)
-			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.stages == 3)
-			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else
-			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		tile_reg_kernel<<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}

@@ -99,11 +99,11 @@ def test_training_learns_a_separable_rule(sb):
     """A rule the features determine (which of 4 feature regions) is learned to >= 95%."""
     S = _sel(sb)
     rng = np.random.default_rng(0)
-    F = np.abs(rng.normal(size=(1200, 10))) + 0.1
+    F = np.abs(rng.normal(size=(3500, 10))) + 0.1
     labels = (F[:, 2] > 0.8).astype(int) * 2 + (F[:, 7] > 0.8).astype(int)
-    sel = S.Selector.train(F[:1000], labels[:1000], epochs=150, batch=100, lr=3e-3, seed=2)
+    sel = S.Selector.train(F[:3000], labels[:3000], epochs=100, batch=100, lr=3e-3, seed=2)
     assert sel.losses[-1] < 0.5 * sel.losses[0]
-    acc = np.mean(sel.predict(F[1000:]) == labels[1000:])
+    acc = np.mean(sel.predict(F[3000:]) == labels[3000:])     # 0.964 with the FP64 oracle
     assert acc >= 0.95, acc
 
 

@@ -76,8 +76,11 @@ def test_rcm_matches_reference(sb, orc, case, expanded):
 
 
 def test_rcm_reduces_bandwidth_and_feeds_every_format(sb, orc):
-    """A scrambled banded matrix: RCM brings its bandwidth back down, and the reordered
-    matrix converts and multiplies in every format like csr_naive does."""
+    """A scrambled banded matrix: RCM brings its bandwidth back down, to the reference's
+    own result, and the reordered matrix converts and multiplies in every format like
+    csr_naive does.  The reference numbers the degree <= 1 vertices first (here 87
+    isolated vertices and a few leaves), so a leaf can land far from its neighbour: its
+    bandwidth on this matrix is 576 (from 3,977), where a textbook RCM reaches about 20."""
     _need(orc)
     rp, ci, v = _lower(4000, 11, band=8)
     full = sb.expand_symmetric(rp, ci, v)[:3]
@@ -90,7 +93,9 @@ def test_rcm_reduces_bandwidth_and_feeds_every_format(sb, orc):
     sci, sv = C[order].astype(np.int32), full[2][order]
     bw = lambda a, c: int(np.max(np.abs(np.repeat(np.arange(m), np.diff(a)) - c)))
     nrp, nci, nv, perm = sb.rcm(srp, sci, sv, symmetry_expanded=True)
-    assert bw(nrp, nci) < bw(srp, sci) / 10
+    r = orc.ref_sym_transform("rcm", srp, sci, sv, expanded=1, threads=1)
+    assert np.array_equal(perm, r[3])
+    assert bw(nrp, nci) == bw(r[0], r[1]) < bw(srp, sci) / 5
     x = np.random.default_rng(2).uniform(-1, 1, m)
     ref = orc.csr_spmv(nrp, nci, nv, x)
     gold, absy = orc.csr_gold(nrp, nci, nv, x)
