@@ -454,9 +454,9 @@ static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
 	return SPMV_OK;
 }
 
-// Kernel choice: -1 = the format's default (the tiled warp-specialised kernel for
-// SELL-C-sigma, the warp-specialised kernel otherwise: the fastest of each on the 4M-row
-// configuration); 0 = CTA
+// Kernel choice: -1 = the format's default (the register-tiled warp kernel for SELL-C-sigma
+// with C = 32, the tiled warp-specialised kernel for wider slices, the warp-specialised
+// kernel otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
 // staged kernel; 1 = direct column-major kernel (slices of >= 32 rows only); 2 =
 // warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
 // block's gather overlapping this block's rows; 4 = warp-specialised staged kernel; 5 = CTA
@@ -464,15 +464,17 @@ static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
 // warp-autonomous kernel whose slice rows load their own x (slices of <= 32 rows); 8 =
 // warp-specialised kernel over the column indices in row-major 8-column tiles (slices of
 // >= 8 rows); 9 = warp-autonomous kernel over the same tiles, x transposed between lanes
-// (slices of exactly 32 rows).
+// (slices of exactly 32 rows); 10 = warps that claim runs of 32-row slices from a queue and
+// sum them from registers, tiles one ahead, x transposed between lanes (no shared memory).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
 	if (k < 0) {
 		// measured on the 4M-row matrix: kernel 4 is the fastest for csr_naive (0.196-0.207 ms),
 		// csr_vec (0.344 against kernel 0's 0.391), sell (0.319 / 0.354) and sell_sorted
-		// (0.341 / 0.371); kernel 8 for SELL-C-sigma (0.255-0.264)
-		k = h.desc.format == SPMV_FMT_SELL_C_S ? 8 : 4;
+		// (0.341 / 0.371); kernel 10 for SELL-C-sigma with C = 32 (0.230 against kernel 8's
+		// 0.255-0.264), kernel 8 for wider slices or a requested staging block
+		k = h.desc.format == SPMV_FMT_SELL_C_S ? (V == 32 && h.desc.block_nnz == 0 ? 10 : 8) : 4;
 		// a requested staging block too large for their two-stage pipeline (about 220 KB of
 		// shared memory per CTA at 12, 16 or 17 bytes an entry) goes to the CTA staged kernel,
 		// which stages fewer blocks at once

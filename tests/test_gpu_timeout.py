@@ -27,7 +27,7 @@ def _matrix(sb):
 @pytest.mark.parametrize("fmt,kw", [
     ("csr_naive", {}),                                  # kernel 4, the csr_naive default
     ("csr_vec", {}),                                    # kernel 4, FMA lanes
-    ("sell_c_s", dict(sellcs_c=32, sellcs_sigma=512)),  # kernel 8 over tiled columns
+    ("sell_c_s", dict(sellcs_c=32, sellcs_sigma=512, kernel=8)),  # kernel 8 over tiled columns
     ("csr_naive", dict(value_type="f32")),              # the FP32 warp-specialised kernel
 ])
 def test_withheld_handoff_times_out_then_fresh_handle_is_exact(sb, orc, fmt, kw):
