@@ -364,9 +364,9 @@ def run_ours(args):
         "config": make_config(args, args.format, m, n, nnz, B, world),
         "gflops": round(head["gflops"], 2),
         "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s",
-                "h2d_bytes_per_step": int(max(0, mf.x_span[1] - mf.x_span[0] + 1) * xh.itemsize),
+                "h2d_bytes_per_step": int((max(0, mf.x_span[1] - mf.x_span[0] + 1) + mf.x_col0) * xh.itemsize),
                 "d2h_bytes_per_step": int(yh.nbytes), "ms_per_step": round(e2e_s * 1e3, 4),
-                "x_span_copied": list(mf.x_span)},
+                "x_copied": {"span": list(mf.x_span), "x0": mf.x_col0}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"

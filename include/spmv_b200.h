@@ -89,11 +89,19 @@ extern "C" {
  *                    a kernel whose wait runs out records SPMV_ERR_TIMEOUT (reported by the
  *                    next spmv_sync() / spmv_run()), waits for its own copies in flight and
  *                    leaves.  0 = about 2 s.                                   default 0
+ *   l2_prefetch      data asked of L2 (cp.async.bulk.prefetch.L2) ahead of the loads that
+ *                    read it: -1 = none; 0 = the kernel's default; k > 0 = k staged blocks
+ *                    ahead of their bulk copies (kernels 4 and 8, the FP32 default).
+ *                    Kernel 10 prefetches the next claimed run of slices and the DIV-RF
+ *                    warp decoder its next packet unless it is -1.  Results are unchanged.
+ *                                                                              default 0
  *   debug_flags      SPMV_DEBUG_WITHHOLD_HANDOFF: the gather warps of the warp-specialised
  *                    kernels (4, 8 and the FP32 default) never hand a stage to the row
  *                    warps, so the row warps' wait runs out: a test of the timeout path
  *                    that faults nothing.                                      default 0
- *   kernel          -1: the format's default (8 for SELL-C-sigma, 4 for the others);
+ *   kernel          -1: the format's default (10 for SELL-C-sigma with C = 32 and no
+ *                       block_nnz, 8 for other SELL-C-sigma, 2 for DIV-RF with 32
+ *                       lanes, 4 for the others);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
  *                    1: direct column-major kernel for slices of >= 32 rows;
  *                    2: warp-autonomous staged kernel (CSR, slices of <= 32 rows);
@@ -115,7 +123,13 @@ extern "C" {
  *                       arrays keep the reference layout);
  *                    9: FP64 slices of exactly 32 rows: kernel 6's warp-owned slices over
  *                       the same tiles; each warp loads x tile by tile and transposes it
- *                       between lanes (no x buffer).                        default -1
+ *                       between lanes (no x buffer);
+ *                   10: FP64 slices of exactly 32 rows: warps claim runs of slices from a
+ *                       queue (the heaviest slices first) and sum them from registers, the
+ *                       next tile's columns and values loaded while this tile is summed,
+ *                       x transposed between lanes (no shared memory).
+ *                    DIV-RF: 0 = one CTA per packet (any lane count), 2 = persistent warps,
+ *                    one lane per lane stream (32 lanes).                     default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;
@@ -137,7 +151,8 @@ typedef struct spmv_format_desc {
 	int32_t debug_flags;
 	int32_t div_packet_reordering;
 	int32_t pack_cols;
-	int32_t reserved[2];
+	int32_t l2_prefetch;
+	int32_t reserved;
 } spmv_format_desc;
 
 #define SPMV_DEBUG_WITHHOLD_HANDOFF 1
@@ -157,8 +172,10 @@ typedef struct spmv_info {
 	char    format_name[64];     /* the reference's format_name, e.g. "Naive_CSR_CPU" -> "Naive_CSR_GPU" */
 	double  alloc_ms;            /* part of convert_ms spent in cudaMalloc                         */
 	double  copy_in_ms;          /* part of convert_ms spent copying the CSR arrays to the device  */
-	int64_t x_lo, x_hi;          /* span of x the converted format reads (its stored columns, padding
-	                                included); spmv_run / spmv_run_f32 copy only x[x_lo..x_hi] */
+	int64_t x_lo, x_hi;          /* span of x the converted format reads: its stored columns other
+	                                than 0, padding included (empty if x_hi < x_lo)              */
+	int64_t x_col0;              /* 1 if a stored column (or a padding entry) is 0.  spmv_run /
+	                                spmv_run_f32 copy only x[0] (if x_col0) and x[x_lo..x_hi]   */
 } spmv_info;
 
 /* Fill *desc with the defaults above for `format`. */

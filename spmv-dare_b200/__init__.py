@@ -123,7 +123,8 @@ class Matrix_Format:
         self.convert_ms = float(info.convert_ms)
         self.alloc_ms = float(info.alloc_ms)
         self.copy_in_ms = float(info.copy_in_ms)
-        self.x_span = (int(info.x_lo), int(info.x_hi))    # the part of x the matrix reads
+        self.x_span = (int(info.x_lo), int(info.x_hi))    # columns above 0 the matrix reads
+        self.x_col0 = bool(info.x_col0)                    # x[0] read too (column 0 or padding)
         self.kernels_per_run = int(info.kernels_per_run)
         self.num_loops = 0
 

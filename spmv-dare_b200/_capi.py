@@ -54,7 +54,7 @@ class FormatDesc(ctypes.Structure):
         ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
         ("stages", c_int32), ("ctas_per_sm", c_int32), ("kernel", c_int32), ("threads", c_int32),
         ("wait_limit_us", c_int32), ("debug_flags", c_int32), ("div_packet_reordering", c_int32),
-        ("pack_cols", c_int32), ("reserved", c_int32 * 2),
+        ("pack_cols", c_int32), ("l2_prefetch", c_int32), ("reserved", c_int32),
     ]
 
 
@@ -64,7 +64,7 @@ class Info(ctypes.Structure):
         ("csr_mem_footprint", c_double), ("stored_elems", c_int64), ("device_bytes", c_int64),
         ("convert_ms", c_double), ("kernels_per_run", c_int32), ("format", c_int32),
         ("format_name", c_char * 64), ("alloc_ms", c_double), ("copy_in_ms", c_double),
-        ("x_lo", c_int64), ("x_hi", c_int64),
+        ("x_lo", c_int64), ("x_hi", c_int64), ("x_col0", c_int64),
     ]
 
 

@@ -93,6 +93,11 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "div_packet_reordering must be 0 or 1 (got %d)", d.div_packet_reordering);
 		return SPMV_ERR_ARG;
 	}
+	if (d.l2_prefetch < -1 || d.l2_prefetch > 64) {
+		set_error(SPMV_ERR_ARG, "l2_prefetch must be -1 (none), 0 (default) or a distance up to 64 (got %d)",
+				d.l2_prefetch);
+		return SPMV_ERR_ARG;
+	}
 	if (d.debug_flags & ~SPMV_DEBUG_WITHHOLD_HANDOFF) {
 		set_error(SPMV_ERR_ARG, "unknown debug_flags bits 0x%x", d.debug_flags);
 		return SPMV_ERR_ARG;
@@ -178,28 +183,37 @@ static int init_device(Handle & h)
 	return SPMV_OK;
 }
 
-// Smallest and largest column index of a stored column array (padding included).
-__global__ void col_span_kernel(const int32_t * c, int64_t n, int * lo_hi)
+// Over a stored column array (padding included): the smallest column other than 0, the
+// largest column, and whether column 0 occurs (the padding column of SELL-C-sigma).
+__global__ void col_span_kernel(const int32_t * c, int64_t n, int * lo_hi_zero)
 {
-	int lo = INT32_MAX, hi = -1;
+	int lo = INT32_MAX, hi = -1, zero = 0;
 	for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
-		lo = min(lo, c[i]);
-		hi = max(hi, c[i]);
+		const int ci = c[i];
+		if (ci == 0)
+			zero = 1;
+		else
+			lo = min(lo, ci);
+		hi = max(hi, ci);
 	}
 	#pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
 		hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+		zero |= __shfl_xor_sync(0xffffffffu, zero, o);
 	}
 	if ((threadIdx.x & 31) == 0) {
-		atomicMin(&lo_hi[0], lo);
-		atomicMax(&lo_hi[1], hi);
+		atomicMin(&lo_hi_zero[0], lo);
+		atomicMax(&lo_hi_zero[1], hi);
+		if (zero)
+			atomicOr(&lo_hi_zero[2], 1);
 	}
 }
 
-// The span of x the converted format reads: the stored column array of the format (SELL's
-// and SELL-C-sigma's padding columns included; DIV-RF reads the CSR columns).  spmv_run
-// copies only that part of a host x to the device.
+// The parts of x the converted format reads, from the stored column array of the format
+// (SELL's and SELL-C-sigma's padding columns included; DIV-RF reads the CSR columns):
+// x[0] if column 0 occurs, and x[x_lo..x_hi] over the other columns.  spmv_run copies only
+// those parts of a host x to the device.
 static int set_x_span(Handle & h)
 {
 	const int32_t * c = h.d_ci;
@@ -213,21 +227,35 @@ static int set_x_span(Handle & h)
 	}
 	h.x_lo = 0;
 	h.x_hi = -1;
+	h.x_col0 = 0;
 	if (cnt <= 0 || h.n <= 0)
 		return SPMV_OK;
 	int * d = nullptr;
-	SPMV_TRY(h.alloc(&d, 2));
-	const int init[2] = {INT32_MAX, -1};
+	SPMV_TRY(h.alloc(&d, 3));
+	const int init[3] = {INT32_MAX, -1, 0};
 	SPMV_CUDA_TRY(cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, h.stream));
 	col_span_kernel<<<(unsigned) (cnt < 256 * 148 * 4 ? ceil_div(cnt, 256) : 148 * 4), 256, 0, h.stream>>>(c, cnt, d);
 	SPMV_CUDA_TRY(cudaGetLastError());
-	int lh[2];
+	int lh[3];
 	SPMV_CUDA_TRY(cudaMemcpyAsync(lh, d, sizeof(lh), cudaMemcpyDeviceToHost, h.stream));
 	SPMV_CUDA_TRY(cudaStreamSynchronize(h.stream));
-	if (lh[1] >= 0) {
+	h.x_col0 = lh[2];
+	if (lh[0] != INT32_MAX) {          // some column above 0
 		h.x_lo = lh[0];
 		h.x_hi = lh[1];
 	}
+	return SPMV_OK;
+}
+
+// Host x -> device: x[0] when column 0 occurs, and x[x_lo..x_hi].
+template <typename T>
+static int copy_x_parts(const Handle & h, T * d_x, const T * x, cudaStream_t s)
+{
+	if (h.x_col0)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(d_x, x, sizeof(T), cudaMemcpyHostToDevice, s));
+	if (h.x_hi >= h.x_lo)
+		SPMV_CUDA_TRY(cudaMemcpyAsync(d_x + h.x_lo, x + h.x_lo, (h.x_hi - h.x_lo + 1) * sizeof(T),
+				cudaMemcpyHostToDevice, s));
 	return SPMV_OK;
 }
 
@@ -466,9 +494,7 @@ int spmv_run(spmv_handle * H, const double * x, double * y)
 		SPMV_TRY(h.alloc(&h.d_y, h.m + 1));
 	}
 	cudaStream_t s = h.stream;
-	if (h.x_hi >= h.x_lo)           // only the span of x the matrix reads
-		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_x + h.x_lo, x + h.x_lo, (h.x_hi - h.x_lo + 1) * sizeof(double),
-				cudaMemcpyHostToDevice, s));
+	SPMV_TRY(copy_x_parts(h, h.d_x, x, s));       // only the parts of x the matrix reads
 	if (h.desc.values == SPMV_VALUES_F32) {
 		// FP32 handle driven with FP64 buffers: round x once, widen y
 		if (!h.d_xf) {
@@ -503,10 +529,7 @@ int spmv_run_f32(spmv_handle * H, const float * x, float * y)
 		SPMV_TRY(h.alloc(&h.d_yf, h.m + 1));
 	}
 	cudaStream_t s = h.stream;
-	if (h.n > 0)
-		if (h.x_hi >= h.x_lo)
-			SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_xf + h.x_lo, x + h.x_lo, (h.x_hi - h.x_lo + 1) * sizeof(float),
-					cudaMemcpyHostToDevice, s));
+	SPMV_TRY(copy_x_parts(h, h.d_xf, x, s));
 	SPMV_TRY(spmv::launch_spmv_f32(h, h.d_xf, h.d_yf, s));
 	if (h.m > 0)
 		SPMV_CUDA_TRY(cudaMemcpyAsync(y, h.d_yf, h.m * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -555,6 +578,7 @@ int spmv_get_info(const spmv_handle * H, spmv_info * out)
 	out->copy_in_ms = h.copy_in_ms;
 	out->x_lo = h.x_lo;
 	out->x_hi = h.x_hi;
+	out->x_col0 = h.x_col0;
 	out->kernels_per_run = h.kernels_per_run;
 	out->format = h.desc.format;
 	snprintf(out->format_name, sizeof(out->format_name), "%s", h.name.c_str());

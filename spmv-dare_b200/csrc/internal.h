@@ -169,7 +169,8 @@ struct Handle {
 	double convert_ms = 0;
 	double alloc_ms = 0;        // host time inside cudaMalloc during the conversion
 	double copy_in_ms = 0;      // the CSR arrays' copy to the device (until it completed)
-	int64_t x_lo = 0, x_hi = -1;  // span of x the converted format reads (inclusive; empty if hi < lo)
+	int64_t x_lo = 0, x_hi = -1;  // span of the format's columns above 0 (inclusive; empty if hi < lo)
+	int64_t x_col0 = 0;           // column 0 occurs (SELL-C-sigma pads with it)
 	int kernels_per_run = 0;
 	std::string name;
 
