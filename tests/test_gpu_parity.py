@@ -144,7 +144,7 @@ def test_warp_specialised_kernel_matches_reference(sb, orc, fmt, threads, block_
 @pytest.mark.parametrize("fmt,kw", [("csr_naive", {}), ("csr_vec", {}), ("sell", {}), ("sell_sorted", {}),
                                     ("sell_c_s", dict(kernel=8)), ("sell_c_s", dict(kernel=4)),
                                     ("sell_c_s", dict(kernel=10))])
-@pytest.mark.parametrize("pf,block_nnz", [(-1, 0), (1, 0), (3, 64), (2, 256)])
+@pytest.mark.parametrize("pf,block_nnz", [(-1, 0), (1, 0), (3, 256), (2, 512)])
 def test_l2_prefetch_does_not_change_results(sb, orc, fmt, kw, pf, block_nnz):
     """Blocks asked of L2 ahead of their bulk copies (kernels 4 and 8), kernel 10's next item:
     the reference's y bits for every distance, small blocks (many prefetched per CTA) included."""
