@@ -89,12 +89,6 @@ extern "C" {
  *                    a kernel whose wait runs out records SPMV_ERR_TIMEOUT (reported by the
  *                    next spmv_sync() / spmv_run()), waits for its own copies in flight and
  *                    leaves.  0 = about 2 s.                                   default 0
- *   l2_prefetch      data asked of L2 (cp.async.bulk.prefetch.L2) ahead of the loads that
- *                    read it: -1 = none; 0 = the kernel's default; k > 0 = k staged blocks
- *                    ahead of their bulk copies (kernels 4 and 8, the FP32 default).
- *                    Kernel 10 prefetches the next claimed run of slices and the DIV-RF
- *                    warp decoder its next packet unless it is -1.  Results are unchanged.
- *                                                                              default 0
  *   debug_flags      SPMV_DEBUG_WITHHOLD_HANDOFF: the gather warps of the warp-specialised
  *                    kernels (4, 8 and the FP32 default) never hand a stage to the row
  *                    warps, so the row warps' wait runs out: a test of the timeout path
@@ -128,8 +122,8 @@ extern "C" {
  *                       queue (the heaviest slices first) and sum them from registers, the
  *                       next tile's columns and values loaded while this tile is summed,
  *                       x transposed between lanes (no shared memory).
- *                    DIV-RF: 0 = one CTA per packet (any lane count), 2 = persistent warps,
- *                    one lane per lane stream (32 lanes).                     default -1
+ *                    DIV-RF: 0 = one CTA per packet (any lane count), 2 = one warp per
+ *                    packet, one lane per lane stream (32 lanes).             default -1
  */
 typedef struct spmv_format_desc {
 	int32_t format;
@@ -151,8 +145,7 @@ typedef struct spmv_format_desc {
 	int32_t debug_flags;
 	int32_t div_packet_reordering;
 	int32_t pack_cols;
-	int32_t l2_prefetch;
-	int32_t reserved;
+	int32_t reserved[2];
 } spmv_format_desc;
 
 #define SPMV_DEBUG_WITHHOLD_HANDOFF 1

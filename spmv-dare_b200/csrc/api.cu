@@ -93,11 +93,6 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "div_packet_reordering must be 0 or 1 (got %d)", d.div_packet_reordering);
 		return SPMV_ERR_ARG;
 	}
-	if (d.l2_prefetch < -1 || d.l2_prefetch > 64) {
-		set_error(SPMV_ERR_ARG, "l2_prefetch must be -1 (none), 0 (default) or a distance up to 64 (got %d)",
-				d.l2_prefetch);
-		return SPMV_ERR_ARG;
-	}
 	if (d.debug_flags & ~SPMV_DEBUG_WITHHOLD_HANDOFF) {
 		set_error(SPMV_ERR_ARG, "unknown debug_flags bits 0x%x", d.debug_flags);
 		return SPMV_ERR_ARG;

@@ -167,23 +167,6 @@ __device__ __forceinline__ void bulk_g2s(void * dst_smem, const void * src_gmem,
 	    : "memory");
 }
 
-// Asks L2 to fetch [p, p + bytes) ahead of its loads: one bulk prefetch (start 16-byte
-// aligned, size a multiple of 16), nothing to wait for, nothing written to shared memory.
-__device__ __forceinline__ void l2_prefetch_bulk(const void * p, uint32_t bytes)
-{
-	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// The 16-byte aligned range [p, p + bytes) prefetched into L2 by the lanes of a warp, in
-// pieces of at most 16 KB (lane i takes pieces i, i + 32, ...).
-__device__ __forceinline__ void warp_l2_prefetch(const void * p, int64_t bytes, int lane)
-{
-	constexpr int64_t PIECE = 16384;
-	const char * c = static_cast<const char *>(p);
-	for (int64_t o = (int64_t) lane * PIECE; o < bytes; o += 32 * PIECE)
-		l2_prefetch_bulk(c + o, (uint32_t) (bytes - o < PIECE ? bytes - o : PIECE));
-}
-
 // Read-only path load of x (L1/texture path, stays in L2 across CTAs).
 template <typename T>
 __device__ __forceinline__ T ldg(const T * p)
@@ -211,14 +194,6 @@ static constexpr long long kWaitBudgetCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 __host__ __device__ __forceinline__ long long wait_budget_cycles(int limit_us)
 {
 	return limit_us > 0 ? (long long) limit_us * 2000LL : kWaitBudgetCycles;
-}
-
-// Staged blocks of the warp-specialised kernels asked of L2 ahead of their bulk copies, for
-// the descriptor's l2_prefetch (-1: none, 0: the default, k > 0: k blocks ahead).
-static constexpr int kWsPrefetchDefault = 0;
-__host__ __forceinline__ int ws_prefetch_distance(int l2_prefetch)
-{
-	return l2_prefetch < 0 ? 0 : l2_prefetch > 0 ? l2_prefetch : kWsPrefetchDefault;
 }
 
 

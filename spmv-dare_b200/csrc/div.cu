@@ -621,7 +621,6 @@ struct DivArgs {
 	int L;
 	const double * x;
 	double * y;
-	int prefetch;            // warp decoder: each warp's next packet prefetched into L2
 };
 
 // Exclusive scan over the threads of each lane (thread t: lane t % L, position t / L in its
@@ -827,10 +826,14 @@ struct LaneReader {
 	}
 };
 
-// Packet p of one warp: its rows summed in ys (the warp's DEC_MAX_ROWS shared doubles), then
-// stored.
-__device__ __forceinline__ void div_warp_packet(const DivArgs & a, int64_t p, int lane, double * ys)
+__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 {
+	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	const int64_t p = (int64_t) blockIdx.x * DIVW_WARPS + wib;
+	if (p >= a.npackets)
+		return;
+	double * ys = ys_all[wib];
 	const uint8_t * h = a.data + a.pkt_off[p];
 	const int64_t nrows = ld_u32(h + 8);
 	const int64_t row_min = ld_u32(h + 12), col_min = ld_u32(h + 16);
@@ -914,34 +917,6 @@ __device__ __forceinline__ void div_warp_packet(const DivArgs & a, int64_t p, in
 		} else {
 			a.y[r] = ys[rel];
 		}
-	}
-}
-
-// The bytes of packet p asked of L2: [pkt_off[p], pkt_off[p + 1]) widened to 16-byte
-// boundaries, which stay inside the allocation (it is 256-byte aligned and carries 16
-// bytes past the last packet).
-__device__ __forceinline__ void div_packet_prefetch(const DivArgs & a, int64_t p, int lane)
-{
-	const int64_t b0 = a.pkt_off[p] & ~(int64_t) 15, b1 = (a.pkt_off[p + 1] + 15) & ~(int64_t) 15;
-	warp_l2_prefetch(a.data + b0, b1 - b0, lane);
-}
-
-// Persistent warps, packets p, p + W, p + 2W, ... (W warps in the grid); with prefetch on,
-// the warp's next packet is asked of L2 before the current one is decoded, so the decode's
-// dependent loads (code byte, payload word, coordinates) hit L2 instead of DRAM.
-__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
-{
-	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
-	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-	const int64_t stride = (int64_t) gridDim.x * DIVW_WARPS;
-	int64_t p = (int64_t) blockIdx.x * DIVW_WARPS + wib;
-	if (a.prefetch && p < a.npackets)
-		div_packet_prefetch(a, p, lane);
-	for (; p < a.npackets; p += stride) {
-		if (a.prefetch && p + stride < a.npackets)
-			div_packet_prefetch(a, p + stride, lane);
-		div_warp_packet(a, p, lane, ys_all[wib]);
-		__syncwarp();                                    // ys read by every lane before it is zeroed again
 	}
 }
 
@@ -1100,16 +1075,6 @@ int convert_div(Handle & h)
 	if (h.exec_kernel != 0 && !(h.exec_kernel == 2 && L == 32)) {
 		set_error(SPMV_ERR_ARG, "DIV-RF: kernel %d unavailable (0, or 2 with vec_len 32)", h.desc.kernel);
 		return SPMV_ERR_ARG;
-	}
-	// the warp decoder's persistent grid: the CTAs the SMs hold at once
-	if (h.exec_kernel == 2) {
-		int per_sm = h.desc.ctas_per_sm;
-		if (per_sm <= 0) {
-			SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, div_warp_kernel, DIVW_WARPS * 32, 0));
-			if (per_sm < 1)
-				per_sm = 1;
-		}
-		h.grid = h.num_sms * per_sm;
 	}
 	// dropped mantissa bits of the lossy mode (reduce_precision, div_kernels_rf.h:467-510)
 	int drop = -1;
@@ -1468,9 +1433,8 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.L = h.desc.vec_len;
 	a.x = d_x;
 	a.y = d_y;
-	a.prefetch = h.desc.l2_prefetch != -1;        // each warp's next packet asked of L2
 	if (h.exec_kernel == 2)
-		div_warp_kernel<<<(unsigned) h.grid, DIVW_WARPS * 32, 0, s>>>(a);
+		div_warp_kernel<<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
 	else
 		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());

@@ -203,7 +203,6 @@ struct F32WsArgs {
 	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
 	const int4 * pinfo;      // packed columns: per block {16-byte offset, base, bits, stream bytes}
 	const uint32_t * pcols;  // packed columns: the streams (pack.cu)
-	int pf;                  // blocks asked of L2 this far ahead of their copies (0: none)
 };
 
 // Column of entry e of a packed block stream (pack.cu): two whole words and a funnel shift.
@@ -234,19 +233,6 @@ __device__ __forceinline__ void f32ws_issue_packed(const F32WsArgs & a, const St
 	mbar_arrive_expect_tx(&bars[s], cnt * 4u + (uint32_t) pi.w);
 	bulk_g2s(st, a.vals + e0, cnt * 4u, &bars[s]);
 	bulk_g2s(words, a.pcols + (int64_t) pi.x * 4, (uint32_t) pi.w, &bars[s]);
-}
-
-// A block's values and columns asked of L2 (the ranges its bulk copy reads, 16-byte
-// aligned), a.pf blocks before that copy is issued.
-__device__ __forceinline__ void f32ws_prefetch(const F32WsArgs & a, const StagedBlock & d)
-{
-	if (d.elems == 0)
-		return;
-	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
-	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
-	const uint32_t cnt = (uint32_t) (e1 - e0);
-	l2_prefetch_bulk(a.vals + e0, cnt * 4u);
-	l2_prefetch_bulk(a.cols + e0, cnt * 4u);
 }
 
 __device__ __forceinline__ void f32ws_issue(const F32WsArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
@@ -358,8 +344,7 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 	}
 	// ---- row warps
 	const int rt = (int) threadIdx.x - ng;
-	const int pf = PACKED ? 0 : a.pf;
-	if (rt == 0) {
+	if (rt == 0)
 		for (int q = 0; q < S; q++) {
 			const int64_t b = b_begin + q;
 			if (b < b_end) {
@@ -374,21 +359,16 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 				}
 			}
 		}
-		for (int q = S; q < S + pf && b_begin + q < b_end; q++)
-			f32ws_prefetch(a, a.blocks[b_begin + q]);
-	}
 	named_bar_sync(1, nr);
 	float ls = 0.0f, lc = 0.0f;      // running Dot2 pair of a long row across its chunks
 	for (int64_t b = b_begin; b < b_end; b++) {
 		const int64_t nb = b + S;
-		StagedBlock dnext{}, dpf{};
+		StagedBlock dnext{};
 		int4 pnext{};
 		if (rt == 0 && nb < b_end) {
 			dnext = a.blocks[nb];
 			if (PACKED)
 				pnext = a.pinfo[nb];
-			if (pf > 0 && nb + pf < b_end)
-				dpf = a.blocks[nb + pf];
 		}
 		const StagedBlock d = sdesc[s];
 		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
@@ -440,8 +420,6 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 			} else {
 				f32ws_issue(a, dnext, s, smem, full);
 			}
-			if (pf > 0 && nb + pf < b_end)
-				f32ws_prefetch(a, dpf);
 		}
 		if (++s == S) {
 			s = 0;
@@ -964,7 +942,6 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 		w.err = h.d_err;
 		w.wait_budget = wait_budget_cycles(h.desc.wait_limit_us);
 		w.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
-		w.pf = ws_prefetch_distance(h.desc.l2_prefetch);
 		w.pinfo = h.d_pinfo;
 		w.pcols = h.d_pcols;
 		if (h.d_pcols)

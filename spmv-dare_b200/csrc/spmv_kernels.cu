@@ -52,7 +52,6 @@ struct StagedArgs {
 	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
 	const int4 * pinfo;      // packed columns (csr_naive): per block {16-byte offset, base, bits, bytes}
 	const uint32_t * pcols;  // packed columns: the block streams (pack.cu)
-	int pf;                  // warp-specialised kernel: blocks asked of L2 this far ahead of their copies (0: none)
 };
 
 // Column of entry e of a packed block stream (pack.cu): two whole words and a funnel shift.
@@ -784,19 +783,6 @@ __device__ __forceinline__ void ws_issue_packed(const StagedArgs & a, const Stag
 	bulk_g2s(sc, a.pcols + (int64_t) pi.x * 4, (uint32_t) pi.w, &bars[s]);
 }
 
-// A block's values and columns asked of L2 (the same 16-byte aligned ranges its bulk copy
-// reads), so that copy, issued a.pf blocks later, lands from L2 instead of DRAM.
-__device__ __forceinline__ void ws_prefetch(const StagedArgs & a, const StagedBlock & d)
-{
-	if (d.elems == 0)
-		return;
-	const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
-	const int64_t e1 = ((int64_t) d.elem0 + d.elems + 3) & ~(int64_t) 3;
-	const uint32_t cnt = (uint32_t) (e1 - e0);
-	l2_prefetch_bulk(a.vals + e0, cnt * 8u);
-	l2_prefetch_bulk(a.cols + e0, cnt * 4u);
-}
-
 __device__ __forceinline__ void ws_issue(const StagedArgs & a, const StagedBlock & d, int s, uint8_t * smem, uint64_t * bars)
 {
 	if (d.elems == 0) {
@@ -965,8 +951,7 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 	}
 	// ---- row warps
 	const int rt = (int) threadIdx.x - ng;
-	const int pf = PK ? 0 : a.pf;
-	if (rt == 0) {
+	if (rt == 0)
 		for (int q = 0; q < S; q++) {
 			const int64_t b = b_begin + q;
 			if (b < b_end) {
@@ -981,9 +966,6 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 				}
 			}
 		}
-		for (int q = S; q < S + pf && b_begin + q < b_end; q++)
-			ws_prefetch(a, a.blocks[b_begin + q]);
-	}
 	named_bar_sync(1, nr);
 	double acc = 0.0;          // running state of a long unit across its chunk blocks
 	double ln[L];
@@ -992,14 +974,12 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 		ln[l] = 0.0;
 	for (int64_t b = b_begin; b < b_end; b++) {
 		const int64_t nb = b + S;
-		StagedBlock dnext{}, dpf{};
+		StagedBlock dnext{};
 		int4 pnext{};
 		if (rt == 0 && nb < b_end) {
 			dnext = a.blocks[nb];
 			if (PK)
 				pnext = a.pinfo[nb];
-			if (pf > 0 && nb + pf < b_end)
-				dpf = a.blocks[nb + pf];
 		}
 		const StagedBlock d = sdesc[s];
 		int js0 = 0, je0 = 0;
@@ -1030,8 +1010,6 @@ __global__ void __launch_bounds__(STAGED_MAX_THREADS) ws_kernel(StagedArgs a)
 			} else {
 				ws_issue(a, dnext, s, smem, full);
 			}
-			if (pf > 0 && nb + pf < b_end)
-				ws_prefetch(a, dpf);
 		}
 		if (++s == S) {
 			s = 0;
@@ -1593,7 +1571,6 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.err = h.d_err;
 	a.wait_budget = wait_budget_cycles(h.desc.wait_limit_us);
 	a.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
-	a.pf = ws_prefetch_distance(h.desc.l2_prefetch);
 	if (fmt == SPMV_FMT_CSR_NAIVE || fmt == SPMV_FMT_CSR_VEC) {
 		a.ptr = h.d_rp;
 		a.cols = h.d_ci;

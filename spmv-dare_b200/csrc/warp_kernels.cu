@@ -429,7 +429,6 @@ struct TileRegArgs {
 	int64_t m;
 	unsigned int * queue;          // [0] next item, [1] warps done: zero at launch, reset on exit
 	unsigned int total_warps;
-	int prefetch;                  // claimed items prefetched into L2 (cp.async.bulk.prefetch)
 };
 
 constexpr int TILE_REG_THREADS = 256;
@@ -492,37 +491,20 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
 }
 
-// The next work item of the warp, its values and tiled columns (contiguous: slices in order,
-// whole 32-row slices, so both ranges are 16-byte aligned) asked of L2 right away.
-__device__ __forceinline__ unsigned int tile_reg_claim(const TileRegArgs & a, int lane)
-{
-	unsigned int it = 0;
-	if (lane == 0)
-		it = atomicAdd(&a.queue[0], 1u);
-	it = __shfl_sync(0xffffffffu, it, 0);
-	if ((int64_t) it < a.nitems && a.prefetch) {
-		const int2 r = a.items[it];
-		const int64_t e0 = a.sptr[r.x], e1 = a.sptr[r.y];
-		warp_l2_prefetch(a.vals + e0, (e1 - e0) * 8, lane);
-		warp_l2_prefetch(a.tcols + e0, (e1 - e0) * 4, lane);
-	}
-	return it;
-}
-
-// Warps claim items one ahead: the item after the current one is claimed, and prefetched
-// into L2, before the current one is summed, so its tiles' DRAM latency overlaps this
-// item's work and the register loads of the tiles hit L2.
 __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
 {
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
-	unsigned int it = tile_reg_claim(a, lane);
-	while ((int64_t) it < a.nitems) {
-		const unsigned int next = tile_reg_claim(a, lane);
+	for (;;) {
+		unsigned int it = 0;
+		if (lane == 0)
+			it = atomicAdd(&a.queue[0], 1u);
+		it = __shfl_sync(0xffffffffu, it, 0);
+		if ((int64_t) it >= a.nitems)
+			break;
 		const int2 r = a.items[it];
 		for (int64_t sl = r.x; sl < r.y; sl++)
 			tile_reg_slice(a, sl, lane, R);
-		it = next;
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
 	// finish puts the queue back to zero for the next launch
@@ -834,7 +816,6 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.m = h.m;
 		a.queue = h.d_queue;
 		a.total_warps = (unsigned int) h.grid * (TILE_REG_THREADS / 32);
-		a.prefetch = h.desc.l2_prefetch != -1;    // the next claimed item asked of L2
 		if (h.desc.format == SPMV_FMT_SELL_C_S) {
 			a.sptr = h.d_sptr32;
 			a.vals = h.d_svals;

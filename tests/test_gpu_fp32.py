@@ -48,17 +48,6 @@ def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
     assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
 
 
-@pytest.mark.parametrize("pf,block_nnz", [(-1, 0), (1, 0), (4, 256)])
-def test_fp32_l2_prefetch_matches_dot2_oracle(sb, orc, pf, block_nnz):
-    """Blocks asked of L2 ahead of their bulk copies: the sequential Dot2 oracle's bits."""
-    for name in golden_names():
-        g = load_golden(name)
-        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
-        mf, y32, y64 = _run(sb, rp, ci, v, x, l2_prefetch=pf, block_nnz=block_nnz)
-        ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
-        assert np.array_equal(y32.view(np.uint32), ref.view(np.uint32)), (name, pf, block_nnz)
-
-
 @pytest.mark.parametrize("block_nnz", [0, 256, 3072])
 def test_fp32_packed_columns_match_dot2_oracle(sb, orc, block_nnz):
     """pack_cols=1: the kernel reads the column indices packed per staged block (smallest

@@ -141,24 +141,6 @@ def test_warp_specialised_kernel_matches_reference(sb, orc, fmt, threads, block_
         assert _eq_bits(y, ref).size == 0, (name, fmt, threads, block_rows, block_nnz, stages)
 
 
-@pytest.mark.parametrize("fmt,kw", [("csr_naive", {}), ("csr_vec", {}), ("sell", {}), ("sell_sorted", {}),
-                                    ("sell_c_s", dict(kernel=8)), ("sell_c_s", dict(kernel=4)),
-                                    ("sell_c_s", dict(kernel=10))])
-@pytest.mark.parametrize("pf,block_nnz", [(-1, 0), (1, 0), (3, 256), (2, 512)])
-def test_l2_prefetch_does_not_change_results(sb, orc, fmt, kw, pf, block_nnz):
-    """Blocks asked of L2 ahead of their bulk copies (kernels 4 and 8), kernel 10's next item:
-    the reference's y bits for every distance, small blocks (many prefetched per CTA) included."""
-    for name in golden_names():
-        g = load_golden(name)
-        mf = _mk(sb, g, fmt, l2_prefetch=pf, block_nnz=0 if kw.get("kernel") == 10 else block_nnz, **kw)
-        y = mf.spmv(g["x"], np.full(mf.m, 1.0))
-        if fmt == "sell_c_s":
-            ref = orc.sellcs_spmv(orc.sellcs_convert(g["row_ptr"], g["col_ind"], g["values"], 32, 512), mf.m, 32, g["x"])
-        else:
-            ref = g[f"y_{fmt}"]
-        assert _eq_bits(y, ref).size == 0, (name, fmt, kw, pf, block_nnz)
-
-
 def test_warp_specialised_kernel_rejects_bad_split(sb):
     g = load_golden("hand6")
     for kw in [dict(threads=64, block_rows=64), dict(threads=128, block_rows=48)]:
@@ -476,13 +458,12 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
         gold, absy = orc.csr_gold(rp, ci, v, x)
         ys = {}
-        for kernel, pf in ((0, 0), (2, 0), (2, -1)):      # the warp decoder with and without its L2 prefetch
-            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel,
-                     l2_prefetch=pf)
+        for kernel in (0, 2):
+            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel)
             for _ in range(2):
-                ys[kernel, pf] = mf.spmv(x, np.full(mf.m, 1.0))
-            assert rel_row_error(ys[kernel, pf], gold, absy) <= TOL, (name, pv, kernel, pf)
-        assert rel_row_error(ys[2, 0], ys[0, 0], absy) <= TOL
+                ys[kernel] = mf.spmv(x, np.full(mf.m, 1.0))
+            assert rel_row_error(ys[kernel], gold, absy) <= TOL, (name, pv, kernel)
+        assert rel_row_error(ys[2], ys[0], absy) <= TOL
     with pytest.raises(sb.SpmvError):
         _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
 
