@@ -43,7 +43,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 CONFIG2 = (4000000, 4000000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7)
-WORKLOAD = "config2: artificial 4Mx4M, avg 20, std 15, gamma, random, bw 0.05, skew 100, neigh 2.0, cross 0.3, seed 7"
+WORKLOAD = "4M-row artificial gamma matrix: 4Mx4M, avg 20, std 15, gamma, random, bw 0.05, skew 100, neigh 2.0, cross 0.3, seed 7"
 FORMATS = ["csr_naive", "csr_vec", "sell", "sell_sorted", "sell_c_s", "div_rf"]
 FORMAT_PARAMS = {
     "sell_c_s": dict(sellcs_c=32, sellcs_sigma=512),
@@ -99,7 +99,7 @@ def hbm_peak():
 
 def ncu_traffic(fmt):
     """dram bytes per launch of the format's kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"spmv_{fmt}_config2.md")
+    p = os.path.join(ROOT, "profiles", f"spmv_{fmt}_gamma4m.md")
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -360,7 +360,7 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32" if f32 else "f64",
-        "data": "synthetic (the reference's artificial generator restated natively, config 2; values 2v-1, x U[-1,1))",
+        "data": "synthetic (the reference's artificial generator restated natively, the 4M-row gamma matrix; values 2v-1, x U[-1,1))",
         "config": make_config(args, args.format, m, n, nnz, B, world),
         "gflops": round(head["gflops"], 2),
         "e2e": {"value": round(world * B * 1e-9 / e2e_s, 2), "unit": "GB/s",
@@ -570,7 +570,7 @@ def cpu_baseline(fmt, rp, ci, v, x, B, sample_s=10.0):
     med = statistics.median(times)
     return {"value": round(B * 1e-9 / med, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
             "format": name, "ms_median": round(med * 1e3, 3),
-            "sample": f"config 2 full matrix, {len(times)} SpMV iterations over ~{sample_s:.0f} s, median"}
+            "sample": f"the full 4M-row matrix, {len(times)} SpMV iterations over ~{sample_s:.0f} s, median"}
 
 
 def run_reference(args):
@@ -610,11 +610,11 @@ def run_reference(args):
         "metric": "SpMV GB/s (algorithmic bytes / time; % of HBM peak in roofline)",
         "value": round(val, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (the reference's own generator, config 2; values 2v-1, x U[-1,1))",
+        "dtype": "f64", "data": "synthetic (the reference's own generator, the 4M-row gamma matrix; values 2v-1, x U[-1,1))",
         "config": make_config(args, name, m, n, nnz, B, world),
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
-                         "sample": f"config 2 full matrix, {args.steps} timed SpMV steps after {args.warmup} warm-up"},
+                         "sample": f"the full 4M-row matrix, {args.steps} timed SpMV steps after {args.warmup} warm-up"},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -854,8 +854,8 @@ def main():
     ap.add_argument("--only-format", dest="all_formats", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--rows", type=int, default=0, help="config 2 with this many rows/cols (profiling)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "batch"])
+    ap.add_argument("--rows", type=int, default=0, help="the 4M-row gamma matrix with this many rows/cols (profiling)")
+    ap.add_argument("--workload", default="gamma4m", choices=["gamma4m", "batch"])
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--retune", action="store_true", help="batch: re-run the autotuner instead of its database")
     ap.add_argument("--no-batch", action="store_true", help="leave the batch block out of the default line")

@@ -1,5 +1,5 @@
 """The native artificial-matrix generator reproduces the reference generator bit for bit
-(golden fixtures made by the reference; config-1 and config-2 regression numbers)."""
+(golden fixtures made by the reference; 100k-row and 4M-row regression numbers)."""
 import numpy as np
 import pytest
 
@@ -22,7 +22,7 @@ def test_generator_matches_reference_fixture(sb, name, threads):
     assert np.array_equal((2.0 * m.values - 1.0).view(np.uint64), g["values"].view(np.uint64))
 
 
-def test_generator_config1_regression(sb):
+def test_generator_normal100k_regression(sb):
     m = sb.generate_artificial(100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14)
     assert m.nnz == 999475
     assert m.stats["max_nnz_per_row"] == 19
@@ -32,7 +32,7 @@ def test_generator_config1_regression(sb):
     assert abs(m.stats["cross_row_similarity"] - 0.455818) < 1e-6
 
 
-def test_generator_config2_regression(sb):
+def test_generator_gamma4m_regression(sb):
     m = sb.generate_artificial(4000000, 4000000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7)
     assert m.nnz == 80469735
     assert m.stats["max_nnz_per_row"] == 2040

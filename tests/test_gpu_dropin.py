@@ -45,7 +45,7 @@ def test_reference_bench_driver_runs_gpu_format(fmt):
 
 def _dropin_matrix(sb):
     """A 20k-row gamma / skewed matrix with empty rows, long rows and 50 columns past the
-    last row (n > m): the config-2 generator parameters at a size the reference runs in
+    last row (n > m): the 4M-row matrix's generator parameters at a size the reference runs in
     well under a second, plus a hand-made tail of every edge the formats pad or split."""
     g = sb.generate_artificial(20000, 20000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7)
     rp, ci = g.row_ptr.astype(np.int64), g.col_ind

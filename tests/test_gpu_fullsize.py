@@ -1,5 +1,5 @@
-"""Full-size parity on the benchmark configurations (config 1: 100k rows, nnz 999,475;
-config 2: 4M rows, nnz 80,469,735), generated by the native generator (itself pinned on
+"""Full-size parity on the benchmark matrices (normal100k: 100k rows, nnz 999,475;
+gamma4m: 4M rows, nnz 80,469,735), generated by the native generator (itself pinned on
 the reference generator) with values mapped v -> 2v - 1 and x ~ U[-1, 1).
 
 Against the reference compiled from its own sources (oracle/_ref, the reference's
@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 T, V = 8, 4
 CONFIGS = {
-    "config1": (100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14),
-    "config2": (4000000, 4000000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7),
+    "normal100k": (100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14),
+    "gamma4m": (4000000, 4000000, 20, 15, "gamma", "random", 0.05, 100, 2.0, 0.3, 7),
 }
 _cache = {}
 
@@ -37,18 +37,18 @@ def _bits(a):
     return np.ascontiguousarray(a, np.float64).view(np.uint64)
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("cfg", ["normal100k", "gamma4m"])
 def test_csr_naive_fullsize(sb, orc, cfg):
     rp, ci, v, x = matrix(sb, cfg)
     mf = sb.csr_to_format(rp, ci, v, format="csr_naive")
-    assert mf.nnz == {"config1": 999475, "config2": 80469735}[cfg]
+    assert mf.nnz == {"normal100k": 999475, "gamma4m": 80469735}[cfg]
     y = mf.spmv(x)
     assert np.array_equal(_bits(y), _bits(orc.csr_spmv(rp, ci, v, x)))
     gold, absy = orc.csr_gold(rp, ci, v, x)
     assert rel_row_error(y, gold, absy) <= TOL
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("cfg", ["normal100k", "gamma4m"])
 def test_csr_naive_packed_columns_fullsize(sb, orc, cfg):
     """csr_naive with packed columns, FP64 and the FP32 variant: the same y bits as the
     plain columns at both sizes."""
@@ -61,7 +61,7 @@ def test_csr_naive_packed_columns_fullsize(sb, orc, cfg):
     assert np.array_equal(y32p.view(np.uint32), y32.view(np.uint32))
 
 
-@pytest.mark.parametrize("cfg,C,sigma", [("config1", 32, 256), ("config2", 32, 512)])
+@pytest.mark.parametrize("cfg,C,sigma", [("normal100k", 32, 256), ("gamma4m", 32, 512)])
 def test_sellcs_fullsize(sb, orc, cfg, C, sigma):
     rp, ci, v, x = matrix(sb, cfg)
     mf = sb.csr_to_format(rp, ci, v, format="sell_c_s", sellcs_c=C, sellcs_sigma=sigma)
@@ -75,8 +75,8 @@ def test_sellcs_fullsize(sb, orc, cfg, C, sigma):
 
 
 @pytest.mark.parametrize("fmt", ["csr_vec", "sell", "sell_sorted"])
-def test_other_formats_config1(sb, orc, fmt):
-    rp, ci, v, x = matrix(sb, "config1")
+def test_other_formats_normal100k(sb, orc, fmt):
+    rp, ci, v, x = matrix(sb, "normal100k")
     mf = sb.csr_to_format(rp, ci, v, format=fmt)
     y = mf.spmv(x)
     if fmt == "csr_vec":
@@ -92,11 +92,11 @@ def test_other_formats_config1(sb, orc, fmt):
 
 
 @pytest.mark.parametrize("fmt", ["sell", "sell_sorted", "csr_vec"])
-def test_other_formats_config2_properties(sb, orc, fmt):
+def test_other_formats_gamma4m_properties(sb, orc, fmt):
     """Config 2 at full size: y bit-identical to the restatement for csr_vec; for the SELL
     pair the layout invariants (pointer monotone, every nnz stored once) and y within the
     tolerance of the binary128 sums."""
-    rp, ci, v, x = matrix(sb, "config2")
+    rp, ci, v, x = matrix(sb, "gamma4m")
     mf = sb.csr_to_format(rp, ci, v, format=fmt)
     y = mf.spmv(x)
     gold, absy = orc.csr_gold(rp, ci, v, x)
@@ -116,7 +116,7 @@ def _need_ref(orc, fmt):
         pytest.fail(f"the compiled reference for {fmt} is missing (make -C oracle ref)")
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("cfg", ["normal100k", "gamma4m"])
 @pytest.mark.parametrize("fmt", ["csr_naive", "csr_vec", "sell", "sell_sorted"])
 def test_against_compiled_reference(sb, orc, cfg, fmt):
     """Converted arrays (row_cluster_ptr, ja, a, thread ranges, permutations) and y bit for
@@ -141,7 +141,7 @@ def test_against_compiled_reference(sb, orc, cfg, fmt):
     assert bad.size == 0, f"{bad.size} rows differ from the reference, first {bad[:5]}"
 
 
-@pytest.mark.parametrize("cfg,C,sigma", [("config1", 32, 256), ("config2", 32, 512)])
+@pytest.mark.parametrize("cfg,C,sigma", [("normal100k", 32, 256), ("gamma4m", 32, 512)])
 def test_sellcs_arrays_against_compiled_reference(sb, orc, cfg, C, sigma):
     """SELL-C-sigma conversion against the reference's own sellcs_format.c / radix_sort.c
     (get_order_by_row_size, csr_to_sellcs), compiled from its sources."""
@@ -159,7 +159,7 @@ def test_sellcs_arrays_against_compiled_reference(sb, orc, cfg, C, sigma):
             assert np.array_equal(got.astype(np.int64), a.astype(np.int64)), k
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("cfg", ["normal100k", "gamma4m"])
 def test_div_rf_against_compiled_reference(sb, orc, cfg):
     """DIV-RF packet bytes and packet-group offsets bit for bit against the reference's
     own compress_kernel_div (div.cpp:236-604, div_kernels_rf.h:538-919) at T = 8, L = 4,
@@ -187,14 +187,14 @@ def test_div_rf_against_compiled_reference(sb, orc, cfg):
     assert rel_row_error(y, gold, absy) <= TOL
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2"])
+@pytest.mark.parametrize("cfg", ["normal100k", "gamma4m"])
 def test_div_rf_fullsize(sb, orc, cfg):
     """Config 1: packet bytes identical to the restatement (itself pinned on the reference
-    at this size); config 2: decode round trip of every packet and y within tolerance."""
+    at this size); gamma4m: decode round trip of every packet and y within tolerance."""
     rp, ci, v, x = matrix(sb, cfg)
     mf = sb.csr_to_format(rp, ci, v, format="div_rf")
     data = mf.export("div_data")
-    if cfg == "config1":
+    if cfg == "normal100k":
         d = orc.div_convert(rp, ci, v, mf.n, T, V, 16384, 0.0)
         assert np.array_equal(data, d["data"])
         assert np.array_equal(mf.export("div_groups"), d["group_pos"])

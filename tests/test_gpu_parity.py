@@ -499,7 +499,7 @@ def test_div_rf_packet_reordering_matches_reference(sb, orc, pv, threads, L, mon
         assert rel_row_error(plain.spmv(x, np.full(mf.m, 1.0)), y, absy) <= TOL
 
 
-def test_div_rf_reordering_config1(sb, orc, monkeypatch):
+def test_div_rf_reordering_normal100k(sb, orc, monkeypatch):
     """The 100k-row configuration with reordering, against the compiled reference."""
     if not orc.ref_available("div_rf"):
         pytest.fail("the compiled reference for div_rf is missing (make -C oracle ref)")

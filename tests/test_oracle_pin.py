@@ -2,7 +2,7 @@
 
 * golden fixtures (tests/golden/, made by make_golden.py from the reference compiled from
   its sources): every converted array and every y, bit for bit;
-* when the reference build is present (oracle/_ref/), the full config-1 matrix
+* when the reference build is present (oracle/_ref/), the full 100k-row matrix
   (100k x 100k, nnz 999,475) as well.
 """
 import numpy as np
@@ -69,7 +69,7 @@ def test_div_round_trip(orc, name):
         assert np.array_equal(_bits(val[order]), _bits(v))
 
 
-def test_restatement_matches_reference_config1(orc):
+def test_restatement_matches_reference_normal100k(orc):
     """Config 1 at full size against the reference compiled from its sources."""
     if not orc.ref_available("div_rf"):
         pytest.skip("reference build (oracle/_ref) not present")
