@@ -347,7 +347,7 @@ def run_ours(args):
 
     value = world * B * 1e-9 / (head["ms_per_step"] * 1e-3)
     achieved = B * 1e-9 / (statistics.median(head["per"]) * 1e-3)
-    traffic = ncu_traffic(args.format)
+    traffic = ncu_traffic("csr_f32_dot2" if f32 else args.format)
     out = {
         "metric": "SpMV GB/s (algorithmic bytes / time; % of HBM peak in roofline)",
         "value": round(value, 2),
@@ -469,7 +469,7 @@ def batch_block(sb, torch, dev, args, world, peak):
     mats, classes, xs, B = batch_matrices(sb, args.batch_count, False)
     xh = np.concatenate(xs)
     xd = torch.from_numpy(xh).to(dev)
-    out = {"workload": BATCH_WORKLOAD, "matrices": len(mats), "bytes_per_step": B,
+    out = {"workload": batch_workload(len(mats)), "matrices": len(mats), "bytes_per_step": B,
            "nnz_total": sum(int(mt[0][-1]) for mt in mats)}
     steps = max(5, args.steps // 2)
     legs = [("tuned", classes), ("mixed", mixed_classes(len(mats)))]
@@ -621,8 +621,12 @@ def run_reference(args):
 
 
 BATCH_SEEDS = (1000, 1512)
-BATCH_WORKLOAD = ("batch: 512 artificial matrices, seeds 1000-1511, rows log-uniform [1e3, 2e5], avg U[5,60], "
+BATCH_WORKLOAD = ("batch: {count} artificial matrices, seeds 1000-{last}, rows log-uniform [1e3, 2e5], avg U[5,60], "
                   "std U[0.1,1]xavg, normal/gamma, skew U[0,200], bw U[0.01,0.5], random placement")
+
+
+def batch_workload(count):
+    return BATCH_WORKLOAD.format(count=count, last=BATCH_SEEDS[0] + count - 1)
 
 
 def batch_matrices(sb, count, retune=False):
@@ -742,7 +746,7 @@ def run_batch(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_graph, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (the reference's artificial generator restated natively; values 2v-1, x U[-1,1))",
-        "config": {"workload": BATCH_WORKLOAD, "matrices": len(mats), "nnz_total": nnz_total, "bytes_per_step": B,
+        "config": {"workload": batch_workload(len(mats)), "matrices": len(mats), "nnz_total": nnz_total, "bytes_per_step": B,
                    "formats": fmt_counts, "tuning": "exhaustive autotuner over the batchable classes",
                    "l2": f"no flush: inputs ({B / 1e9:.2f} GB/step) exceed the 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -834,7 +838,7 @@ def run_reference_batch(args):
         "value": round(val, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (the reference's artificial generator restated natively; values 2v-1, x U[-1,1))",
-        "config": {"workload": BATCH_WORKLOAD, "matrices": len(mats), "bytes_per_step": B, "format": "csr_naive"},
+        "config": {"workload": batch_workload(len(mats)), "matrices": len(mats), "bytes_per_step": B, "format": "csr_naive"},
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
                          "sample": f"all {len(mats)} matrices per step; each matrix converted, its SpMV timed "
