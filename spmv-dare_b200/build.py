@@ -31,12 +31,14 @@ if not os.path.exists(NVCC):
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-I" + INCLUDE, "-I" + CSRC,
                      "--expt-relaxed-constexpr", "-diag-suppress", "177"]
-GCC_FLAGS = ["-O3", "-march=x86-64-v3", "-fPIC", "-fopenmp", "-std=gnu11", "-Wall", "-Wno-unused-result"]
+CUDA_INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(NVCC))), "include")
+GCC_FLAGS = ["-O3", "-march=x86-64-v3", "-fPIC", "-fopenmp", "-std=gnu11", "-Wall", "-Wno-unused-result",
+             "-I" + CUDA_INCLUDE]
 
 CU_SOURCES = ["primitives.cu", "convert.cu", "spmv_kernels.cu", "warp_kernels.cu", "div.cu", "fp32.cu", "batch.cu", "select.cu",
               "mtx.cu", "pack.cu", "sym.cu", "gen.cu", "api.cu"]
-C_SOURCES = ["artgen.c", "mtx_parse.c"]
-HEADERS = ["common.cuh", "primitives.cuh", "internal.h", "mtx_parse.h"]
+C_SOURCES = ["artgen.c", "mtx_parse.c", "hostcopy.c"]
+HEADERS = ["common.cuh", "primitives.cuh", "internal.h", "mtx_parse.h", "hostcopy.h"]
 
 
 def _newer(src_list, target):
@@ -71,7 +73,7 @@ def build(verbose=False, jobs=None):
         src = os.path.join(CSRC, s)
         obj = os.path.join(OBJ, s + ".o")
         objs.append(obj)
-        if _newer([src], obj):
+        if _newer([src] + headers, obj):
             steps.append(["gcc"] + GCC_FLAGS + ["-c", src, "-o", obj])
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
         for out in ex.map(_run, steps):

@@ -5,6 +5,7 @@
 #include <chrono>
 #include <string>
 
+#include "hostcopy.h"
 #include "internal.h"
 #include "primitives.cuh"
 
@@ -316,10 +317,11 @@ static int create_common(Handle & h, const int32_t * rp, const int32_t * ci, con
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_v + nnz, 0, SPMV_ENTRY_PAD * sizeof(double), s));
 	const auto tc = std::chrono::steady_clock::now();
 	if (host) {
-		SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_rp, rp, (m + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+		// pageable host arrays: large ones go through the pinned staging copy
+		SPMV_CUDA_TRY(spmv_h2d_pageable(h.d_rp, rp, (m + 1) * sizeof(int32_t), s));
 		if (nnz > 0) {
-			SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_ci, ci, nnz * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-			SPMV_CUDA_TRY(cudaMemcpyAsync(h.d_v, v, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+			SPMV_CUDA_TRY(spmv_h2d_pageable(h.d_ci, ci, nnz * sizeof(int32_t), s));
+			SPMV_CUDA_TRY(spmv_h2d_pageable(h.d_v, v, nnz * sizeof(double), s));
 		}
 	} else {
 		if (user_stream) {

@@ -444,7 +444,25 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
-__device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int lane, int R)
+// PF 1 / 2: the cache lines of the entries two tiles ahead (512 entries on, across slice
+// boundaries: an item's slices are contiguous; never past the item's end e_end) requested
+// into L1 / L2 by one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the 1 KB of
+// columns), so the next tile's register loads find them close.
+template <int PF>
+__device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0, int64_t e_end, int lane)
+{
+	const int64_t p = t0 + 512;
+	if (PF == 0 || lane >= 24 || p + 256 > e_end)
+		return;
+	const void * addr = lane < 16 ? (const void *) (a.vals + p + lane * 16) : (const void *) (a.tcols + p + (lane - 16) * 32);
+	if (PF == 1)
+		asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
+	else
+		asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
+}
+
+template <int PF>
+__device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R)
 {
 	const int64_t b = a.sptr[sl];
 	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
@@ -455,6 +473,7 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 	if (nt > 0)
 		tile_load(a, b, lane, R, c, v);
 	for (int t = 0; t < nt; t++) {
+		tile_prefetch<PF>(a, b + (int64_t) t * 256, e_end, lane);
 		if (t + 1 < nt)
 			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, cn, vn);
 		double X[8];
@@ -491,6 +510,7 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
 }
 
+template <int PF>
 __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
 {
 	const int lane = threadIdx.x & 31;
@@ -503,8 +523,9 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 		if ((int64_t) it >= a.nitems)
 			break;
 		const int2 r = a.items[it];
+		const int64_t e_end = a.sptr[r.y];
 		for (int64_t sl = r.x; sl < r.y; sl++)
-			tile_reg_slice(a, sl, lane, R);
+			tile_reg_slice<PF>(a, sl, e_end, lane, R);
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
 	// finish puts the queue back to zero for the next launch
@@ -791,7 +812,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<0>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -825,7 +846,13 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		tile_reg_kernel<<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		// stages 3 / 4: lines two tiles ahead prefetched into L1 / L2
+		if (h.desc.stages == 3)
+			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 4)
+			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else
+			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}
