@@ -461,6 +461,47 @@ __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0,
 		asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
 }
 
+// x of one full tile (lane L's 8 tiled positions), transposed so that lane L holds its row's
+// 8 values, and the row's FMA chain continued over them in column order.
+__device__ __forceinline__ double tile_sum(const TileRegArgs & a, const int32_t (&c)[8], const double (&v)[8], int lane,
+		double acc)
+{
+	double X[8];
+	#pragma unroll
+	for (int q = 0; q < 8; q++)
+		X[q] = __ldg(a.x + c[q]);
+	transpose8(X, lane);
+	#pragma unroll
+	for (int j = 0; j < 8; j++)
+		acc = __fma_rn(v[j], X[j], acc);
+	return acc;
+}
+
+// PF 3: the full tiles through two fixed register slots, the loop unrolled by two, so the
+// next tile's loads land in the slot the previous iteration consumed (no register moves of
+// data still in flight).
+template <int PF>
+__device__ __forceinline__ double tile_reg_full_tiles(const TileRegArgs & a, int64_t b, int nt, int lane, int R)
+{
+	double acc = 0.0;
+	int32_t c0[8], c1[8];
+	double v0[8], v1[8];
+	if (nt > 0)
+		tile_load(a, b, lane, R, c0, v0);
+	for (int t = 0; t < nt;) {
+		if (t + 1 < nt)
+			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, c1, v1);
+		acc = tile_sum(a, c0, v0, lane, acc);
+		if (++t >= nt)
+			break;
+		if (t + 1 < nt)
+			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, c0, v0);
+		acc = tile_sum(a, c1, v1, lane, acc);
+		++t;
+	}
+	return acc;
+}
+
 template <int PF>
 __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R)
 {
@@ -470,9 +511,11 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 	double acc = 0.0;
 	int32_t c[8], cn[8];
 	double v[8], vn[8];
-	if (nt > 0)
+	if (PF == 3)
+		acc = tile_reg_full_tiles<PF>(a, b, nt, lane, R);
+	else if (nt > 0)
 		tile_load(a, b, lane, R, c, v);
-	for (int t = 0; t < nt; t++) {
+	for (int t = 0; PF != 3 && t < nt; t++) {
 		tile_prefetch<PF>(a, b + (int64_t) t * 256, e_end, lane);
 		if (t + 1 < nt)
 			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, cn, vn);
@@ -851,6 +894,8 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 5)          // two fixed register slots, loop unrolled by two
+			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
 			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());

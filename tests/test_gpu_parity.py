@@ -242,12 +242,13 @@ def test_tiled_kernel_long_slices(sb, orc):
                 assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
-@pytest.mark.parametrize("stages", [0, 3, 4])
+@pytest.mark.parametrize("stages", [0, 3, 4, 5])
 @pytest.mark.parametrize("fmt,C,sigma", [("sell_c_s", 32, 512), ("sell_c_s", 32, 32), ("sell_c_s", 32, 4096),
                                          ("sell", 32, 0), ("sell_sorted", 32, 0), ("sell_c_s", 64, 512)])
 def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma, stages):
     """Kernel 10 (warp-claimed slices of 32 rows summed from registers, no shared memory;
-    stages 3 / 4 add a prefetch of the lines two tiles ahead into L1 / L2):
+    stages 3 / 4 add a prefetch of the lines two tiles ahead into L1 / L2, stages 5 runs the
+    full tiles through two fixed register slots):
     the reference's y bits on every golden case and on a skewed matrix whose heavy slices
     (rows up to 3,000 entries) are claimed first; slice heights other than 32 fall back to
     kernel 8.  Several launches in a row reuse the work queue, which each launch resets."""
