@@ -106,7 +106,7 @@ def main(argv=None):
     ap.add_argument("--train", default=os.path.join(HERE, "data", "tune_selector_train.npz"))
     ap.add_argument("--test", default=os.path.join(HERE, "data", "tune_selector_test.npz"))
     ap.add_argument("--out", default=None)
-    ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--near", type=float, default=0.01)
     a = ap.parse_args(argv)
     sys.path.insert(0, HERE)
