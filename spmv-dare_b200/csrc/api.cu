@@ -107,7 +107,7 @@ static int check_desc(const spmv_format_desc & d)
 		return SPMV_ERR_ARG;
 	}
 	if (d.block_nnz < 0 || d.block_nnz > 16384 || d.stages < 0 || d.stages > 8 || d.block_rows < 0 ||
-			d.block_rows > 4096 || d.ctas_per_sm < 0 || d.ctas_per_sm > 32 || d.kernel < -1 || d.kernel > 11 ||
+			d.block_rows > 4096 || d.ctas_per_sm < 0 || d.ctas_per_sm > 32 || d.kernel < -1 || d.kernel > 10 ||
 			!(d.threads == 0 || (d.threads % 32 == 0 && d.threads >= 64 && d.threads <= 512))) {
 		set_error(SPMV_ERR_ARG, "tuning knob out of range");
 		return SPMV_ERR_ARG;
@@ -116,8 +116,8 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "kernel 7 (segmented) is the FP32 variant's kernel");
 		return SPMV_ERR_ARG;
 	}
-	if (d.kernel >= 8 && d.values != SPMV_VALUES_F64) {
-		set_error(SPMV_ERR_ARG, "kernels 8 to 11 (tiled slices) run FP64 values");
+	if ((d.kernel == 8 || d.kernel == 9 || d.kernel == 10) && d.values != SPMV_VALUES_F64) {
+		set_error(SPMV_ERR_ARG, "kernels 8, 9 and 10 (tiled slices) run FP64 values");
 		return SPMV_ERR_ARG;
 	}
 	return SPMV_OK;

@@ -420,12 +420,12 @@ int validate_csr(Handle & h)
 	return SPMV_OK;
 }
 
-// Column indices of the slices in row-major tiles of TW slice columns (TW = 8: kernels
-// 8-10; TW = 4: kernel 11).  Entry (row r, column k) of slice s, width W = (P[s + 1] -
-// P[s]) / V, moves from P[s] + k * V + r to P[s] + k8 * V + r * tw + (k - k8), k8 = k & -TW,
-// tw = min(TW, W - k8): a permutation inside every slice, so blocks of whole slices and
-// chunks of whole tiles are contiguous ranges of the tiled array too.  One thread per slice row.
-__global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, int TW, const int32_t * cols, int32_t * out)
+// Column indices of the slices in row-major tiles of 8 slice columns (kernel 8).  Entry
+// (row r, column k) of slice s, width W = (P[s + 1] - P[s]) / V, moves from
+// P[s] + k * V + r to P[s] + k8 * V + r * tw + (k - k8), k8 = k & ~7, tw = min(8, W - k8):
+// a permutation inside every slice, so blocks of whole slices and chunks of whole tiles
+// are contiguous ranges of the tiled array too.  One thread per slice row.
+__global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, const int32_t * cols, int32_t * out)
 {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= ns * V)
@@ -435,20 +435,20 @@ __global__ void tile_cols_kernel(const int32_t * P, int64_t ns, int V, int TW, c
 	const int64_t b = P[sl];
 	const int W = (int) (((int64_t) P[sl + 1] - b) / V);
 	for (int k = 0; k < W; k++) {
-		const int k8 = k & -TW;
-		const int tw = W - k8 < TW ? W - k8 : TW;
+		const int k8 = k & ~7;
+		const int tw = W - k8 < 8 ? W - k8 : 8;
 		out[b + (int64_t) k8 * V + (int64_t) r * tw + (k - k8)] = cols[b + (int64_t) k * V + r];
 	}
 }
 
 // The tiled copy of a sliced format's column indices (kernels 8 and 9).
-static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V, int tw = 8)
+static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	const int32_t * cols = h.desc.format == SPMV_FMT_SELL_C_S ? h.d_scols : h.d_ja;
 	SPMV_TRY(h.alloc(&h.d_tcols, h.stored_elems + 8));
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_tcols, 0, (h.stored_elems + 8) * sizeof(int32_t), h.stream));
 	if (U > 0) {
-		tile_cols_kernel<<<(unsigned) ceil_div(U * V, 256), 256, 0, h.stream>>>(d_P, U, V, tw, cols, h.d_tcols);
+		tile_cols_kernel<<<(unsigned) ceil_div(U * V, 256), 256, 0, h.stream>>>(d_P, U, V, cols, h.d_tcols);
 		SPMV_CUDA_TRY(cudaGetLastError());
 	}
 	return SPMV_OK;
@@ -465,8 +465,7 @@ static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V, i
 // warp-specialised kernel over the column indices in row-major 8-column tiles (slices of
 // >= 8 rows); 9 = warp-autonomous kernel over the same tiles, x transposed between lanes
 // (slices of exactly 32 rows); 10 = warps that claim runs of 32-row slices from a queue and
-// sum them from registers, tiles one ahead, x transposed between lanes (no shared memory);
-// 11 = kernel 10 over 4-column tiles, three tiles in flight through four register slots.
+// sum them from registers, tiles one ahead, x transposed between lanes (no shared memory).
 int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
@@ -491,7 +490,7 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		k = 2;                      // CSR: the warp kernel's own path
 	if (k == 8 && V < 8)
 		k = 4;                      // narrower slices already give a warp 8 neighbouring columns
-	if ((k == 9 || k == 10 || k == 11) && V != 32)
+	if ((k == 9 || k == 10) && V != 32)
 		k = V >= 8 ? 8 : 4;         // kernels 9 and 10's lane transpose takes slices of exactly 32 rows
 	if (k == 10 && V == 1)
 		k = 4;
@@ -504,8 +503,8 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 		SPMV_TRY(build_tiled_cols(h, d_P, U, V));
 		return build_warp_chunks(h, d_P, U, V);
 	}
-	if (k == 10 || k == 11) {
-		SPMV_TRY(build_tiled_cols(h, d_P, U, V, k == 11 ? 4 : 8));
+	if (k == 10) {
+		SPMV_TRY(build_tiled_cols(h, d_P, U, V));
 		return build_tile_reg(h, d_P, U, V);
 	}
 	staged_defaults(h);

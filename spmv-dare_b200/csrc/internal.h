@@ -104,7 +104,7 @@ struct Handle {
 	                             // own-gather, 6 warp-autonomous own-gather, 7 FP32 segmented,
 	                             // 8 warp-specialised over tiled slice columns
 	int row_threads = 0;         // kernels 4 and 8: threads of the row warps (the rest gather)
-	int32_t * d_tcols = nullptr; // kernels 8-11: slice column indices, row-major in 8-column (11: 4-column) tiles
+	int32_t * d_tcols = nullptr; // kernels 8-10: slice column indices, row-major in 8-column tiles
 	int2 * d_items = nullptr;    // kernel 10: work items (slice ranges), heaviest first
 	int64_t num_items = 0;
 	unsigned int * d_queue = nullptr;  // kernel 10: work-queue head and finished-warp count

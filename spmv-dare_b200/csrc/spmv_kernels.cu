@@ -1515,7 +1515,7 @@ int launch_spmv(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	const int fmt = h.desc.format;
 	if (fmt == SPMV_FMT_DIV_RF)
 		return launch_div(h, d_x, d_y, s);
-	if (h.exec_kernel == 2 || h.exec_kernel == 6 || h.exec_kernel == 9 || h.exec_kernel == 10 || h.exec_kernel == 11)
+	if (h.exec_kernel == 2 || h.exec_kernel == 6 || h.exec_kernel == 9 || h.exec_kernel == 10)
 		return launch_warp(h, d_x, d_y, s);
 	if (h.exec_kernel == 1) {
 		SlicedArgs a{};

@@ -814,134 +814,6 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 	return SPMV_OK;
 }
 
-// ------------------------------------------------------------------ kernel 11: 4-column tiles
-// Kernel 10's work items and queue over a copy of the columns in row-major tiles of 4 slice
-// columns (128 entries).  Lane L loads tiled positions q * 32 + L (q = 0..3): row 8q + L/4,
-// column L % 4; a 4 x 4 transpose inside each group of 4 lanes leaves lane L with row
-// R4 = 8 (L % 4) + L / 4, columns 0..3, whose values it loads column-major (a permutation of
-// the slice's 32 rows per column: 256 contiguous bytes a warp load).  A tile takes 12
-// registers (4 columns, 4 values), so four fixed register slots hold the tile being summed
-// and the next three in flight (4.5 KB a warp), the loop unrolled by four so no slot is
-// copied while its loads are in flight.
-
-__device__ __forceinline__ void tile4_load(const TileRegArgs & a, int64_t t0, int lane, int R4, int32_t (&c)[4],
-		double (&v)[4])
-{
-	#pragma unroll
-	for (int q = 0; q < 4; q++)
-		c[q] = __ldcs(a.tcols + t0 + q * 32 + lane);
-	#pragma unroll
-	for (int j = 0; j < 4; j++)
-		v[j] = __ldcs(a.vals + t0 + j * 32 + R4);
-}
-
-// X[i] of lane j (of a group of 4) is element (i, j); afterwards X[i] is element (j, i).  Per
-// lane bit m: lanes l and l ^ m swap element i1 of the lower and element i0 of the upper lane
-// for each index pair (i0, i1 = i0 | m).
-__device__ __forceinline__ void transpose4(double (&X)[4], int lane)
-{
-	#pragma unroll
-	for (int m = 1; m <= 2; m <<= 1) {
-		const bool hi = (lane & m) != 0;
-		#pragma unroll
-		for (int i0 = 0; i0 < 4; i0++) {
-			if (i0 & m)
-				continue;
-			const int i1 = i0 | m;
-			const double send = hi ? X[i0] : X[i1];
-			const double recv = __shfl_xor_sync(0xffffffffu, send, m);
-			if (hi)
-				X[i0] = recv;
-			else
-				X[i1] = recv;
-		}
-	}
-}
-
-__device__ __forceinline__ double tile4_sum(const TileRegArgs & a, const int32_t (&c)[4], const double (&v)[4], int lane,
-		double acc)
-{
-	double X[4];
-	#pragma unroll
-	for (int q = 0; q < 4; q++)
-		X[q] = __ldg(a.x + c[q]);
-	transpose4(X, lane);
-	#pragma unroll
-	for (int j = 0; j < 4; j++)
-		acc = __fma_rn(v[j], X[j], acc);
-	return acc;
-}
-
-__device__ __forceinline__ void tile4_slice(const TileRegArgs & a, int64_t sl, int lane, int R4)
-{
-	const int64_t b = a.sptr[sl];
-	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
-	const int nt = W >> 2, rem = W & 3;
-	double acc = 0.0;
-	int32_t c0[4], c1[4], c2[4], c3[4];
-	double v0[4], v1[4], v2[4], v3[4];
-	if (nt > 0)
-		tile4_load(a, b, lane, R4, c0, v0);
-	if (nt > 1)
-		tile4_load(a, b + 128, lane, R4, c1, v1);
-	if (nt > 2)
-		tile4_load(a, b + 256, lane, R4, c2, v2);
-	// step: tile t + 3 into slot N, then tile t (slot C) summed
-#define TILE4_STEP(C, VC, N, VN)                                                \
-	if (t + 3 < nt)                                                             \
-		tile4_load(a, b + (int64_t) (t + 3) * 128, lane, R4, N, VN);             \
-	acc = tile4_sum(a, C, VC, lane, acc);                                       \
-	if (++t >= nt)                                                              \
-		break;
-	for (int t = 0; t < nt;) {
-		TILE4_STEP(c0, v0, c3, v3)
-		TILE4_STEP(c1, v1, c0, v0)
-		TILE4_STEP(c2, v2, c1, v1)
-		TILE4_STEP(c3, v3, c2, v2)
-	}
-#undef TILE4_STEP
-	if (rem > 0) {                               // the narrower last tile: rows at R4 * rem
-		const int64_t t0 = b + (int64_t) nt * 128;
-		double X[4], vv[4];
-		#pragma unroll
-		for (int j = 0; j < 4; j++) {
-			if (j < rem) {
-				X[j] = __ldg(a.x + __ldcs(a.tcols + t0 + R4 * rem + j));
-				vv[j] = __ldcs(a.vals + t0 + j * 32 + R4);
-			}
-		}
-		#pragma unroll
-		for (int j = 0; j < 4; j++)
-			if (j < rem)
-				acc = __fma_rn(vv[j], X[j], acc);
-	}
-	const int64_t row = sl * 32 + R4;
-	if (row < a.m)
-		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(TILE_REG_THREADS, MINB) tile4_kernel(TileRegArgs a)
-{
-	const int lane = threadIdx.x & 31;
-	const int R4 = 8 * (lane & 3) + (lane >> 2);
-	for (;;) {
-		unsigned int it = 0;
-		if (lane == 0)
-			it = atomicAdd(&a.queue[0], 1u);
-		it = __shfl_sync(0xffffffffu, it, 0);
-		if ((int64_t) it >= a.nitems)
-			break;
-		const int2 r = a.items[it];
-		for (int64_t sl = r.x; sl < r.y; sl++)
-			tile4_slice(a, sl, lane, R4);
-	}
-	if (lane == 0 && atomicAdd(&a.queue[1], 1u) == a.total_warps - 1) {
-		atomicExch(&a.queue[0], 0u);
-		atomicExch(&a.queue[1], 0u);
-	}
-}
-
 // Work items of kernel 10: slices of at least TILE_REG_HEAVY entries alone, the heaviest
 // first; the others in matrix order, in runs of consecutive slices of about
 // TILE_REG_ITEM entries (neighbouring rows keep x warm in L2).
@@ -950,7 +822,7 @@ constexpr int64_t TILE_REG_HEAVY = 4096, TILE_REG_ITEM = 2048;
 int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	if (V != 32) {
-		set_error(SPMV_ERR_ARG, "kernels 10 and 11 take slices of exactly 32 rows (got %d)", V);
+		set_error(SPMV_ERR_ARG, "kernel 10 takes slices of exactly 32 rows (got %d)", V);
 		return SPMV_ERR_ARG;
 	}
 	cudaStream_t s = h.stream;
@@ -983,10 +855,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		const void * fn = (const void *) tile_reg_kernel<0>;
-		if (h.exec_kernel == 11)
-			fn = h.desc.stages == 2 ? (const void *) tile4_kernel<2> : (const void *) tile4_kernel<3>;
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<0>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -999,7 +868,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 
 int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 {
-	if (h.exec_kernel == 10 || h.exec_kernel == 11) {
+	if (h.exec_kernel == 10) {
 		if (h.num_items == 0)
 			return SPMV_OK;
 		TileRegArgs a{};
@@ -1021,12 +890,7 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
 		// stages 3 / 4: lines two tiles ahead prefetched into L1 / L2
-		if (h.exec_kernel == 11) {             // 3 CTAs an SM at 80 registers; stages 2: 2 CTAs at 96
-			if (h.desc.stages == 2)
-				tile4_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-			else
-				tile4_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		} else if (h.desc.stages == 3)
+		if (h.desc.stages == 3)
 			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);

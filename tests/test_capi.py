@@ -60,8 +60,7 @@ def test_symmetric_unexpanded_is_rejected(sb):
     (dict(format="csr_naive", kernel=7), 1),                      # the segmented kernel is FP32 only
     (dict(format="csr_naive", kernel=8, value_type="f32"), 1),    # the tiled kernels are FP64 only
     (dict(format="csr_naive", kernel=9, value_type="f32"), 1),
-    (dict(format="sell_c_s", kernel=12), 1),
-    (dict(format="sell_c_s", kernel=11, value_type="f32"), 1),
+    (dict(format="sell_c_s", kernel=11), 1),
     (dict(format="sell_c_s", kernel=10, value_type="f32"), 1),   # kernel 10 is FP64 slices
     (dict(format="csr_naive", wait_limit_us=-5), 1),
     (dict(format="csr_naive", debug_flags=4), 1),
