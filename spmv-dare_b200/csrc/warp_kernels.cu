@@ -429,6 +429,7 @@ struct TileRegArgs {
 	int64_t m;
 	unsigned int * queue;          // [0] next item, [1] warps done: zero at launch, reset on exit
 	unsigned int total_warps;
+	int pf_dist;                   // line prefetch distance in entries (a multiple of 256)
 };
 
 constexpr int TILE_REG_THREADS = 256;
@@ -444,14 +445,14 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
-// PF 1 / 2: the cache lines of the entries two tiles ahead (512 entries on, across slice
-// boundaries: an item's slices are contiguous; never past the item's end e_end) requested
-// into L1 / L2 by one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the 1 KB of
-// columns), so the next tile's register loads find them close.
+// PF 1 / 2: the cache lines of the tile pf_dist entries ahead (two tiles by default; across
+// slice boundaries: an item's slices are contiguous; never past the item's end e_end)
+// requested into L1 / L2 by one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the
+// 1 KB of columns), so that tile's register loads find them close.
 template <int PF>
 __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0, int64_t e_end, int lane)
 {
-	const int64_t p = t0 + 512;
+	const int64_t p = t0 + a.pf_dist;
 	if (PF == 0 || lane >= 24 || p + 256 > e_end)
 		return;
 	const void * addr = lane < 16 ? (const void *) (a.vals + p + lane * 16) : (const void *) (a.tcols + p + (lane - 16) * 32);
@@ -816,7 +817,8 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 
 // Work items of kernel 10: slices of at least TILE_REG_HEAVY entries alone, the heaviest
 // first; the others in matrix order, in runs of consecutive slices of about
-// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2).
+// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2); block_rows sets the item
+// size in 256-entry tiles instead (the heavy threshold is twice the item size).
 constexpr int64_t TILE_REG_HEAVY = 4096, TILE_REG_ITEM = 2048;
 
 int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
@@ -830,16 +832,18 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemcpyAsync(P.data(), d_P, (U + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
 	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
 	std::vector<int2> heavy, rest;
+	const int64_t item = h.desc.block_rows > 0 ? (int64_t) h.desc.block_rows * 256 : TILE_REG_ITEM;
+	const int64_t heavy_min = h.desc.block_rows > 0 ? 2 * item : TILE_REG_HEAVY;
 	int64_t u = 0;
 	while (u < U) {
 		const int64_t len = (int64_t) P[u + 1] - P[u];
-		if (len >= TILE_REG_HEAVY) {
+		if (len >= heavy_min) {
 			heavy.push_back(make_int2((int) u, (int) (u + 1)));
 			u++;
 			continue;
 		}
 		const int64_t u0 = u, e0 = P[u];
-		while (u < U && (int64_t) P[u + 1] - P[u] < TILE_REG_HEAVY && (int64_t) P[u] - e0 < TILE_REG_ITEM)
+		while (u < U && (int64_t) P[u + 1] - P[u] < heavy_min && (int64_t) P[u] - e0 < item)
 			u++;
 		rest.push_back(make_int2((int) u0, (int) u));
 	}
@@ -880,6 +884,8 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.m = h.m;
 		a.queue = h.d_queue;
 		a.total_warps = (unsigned int) h.grid * (TILE_REG_THREADS / 32);
+		// block_nnz: the line prefetch distance in entries (whole tiles; default two tiles)
+		a.pf_dist = h.desc.block_nnz > 0 ? (int) (ceil_div(h.desc.block_nnz, 256) * 256) : 512;
 		if (h.desc.format == SPMV_FMT_SELL_C_S) {
 			a.sptr = h.d_sptr32;
 			a.vals = h.d_svals;
