@@ -21,8 +21,8 @@ from its sources (oracle/_ref), on all host cores.
 
 --workload batch: the batched engine on 512 artificial matrices (seeds 1000-1511, rows
 log-uniform in [1e3, 2e5], parameters from spmv-dare_b200/workloads.py), each in the format
-the exhaustive autotuner picked for it (spmv-dare_b200/data/tune_batch.npz; --retune
-re-runs the autotuner here).  A step is one SpMV of every matrix: one CUDA-graph replay of
+the batch autotuner picked for it from the matrices' exhaustive timings
+(spmv-dare_b200/data/tune_batch.npz, tuning.batch_plan; --retune re-runs the timings here).  A step is one SpMV of every matrix: one CUDA-graph replay of
 the persistent work-queue kernel (`value`), beside the same batch launched directly and the
 512 matrices launched one by one with their own handles.  Metric: the aggregate algorithmic
 bytes of the 512 SpMVs over the step time.
@@ -635,26 +635,29 @@ def batch_matrices(sb, count, retune=False):
     sys.path.insert(0, pkg)
     from spmv_dare_b200 import tuning, workloads
 
-    best = {}
+    times = {}
     db_path = os.path.join(pkg, "data", "tune_batch.npz")
     if not retune and os.path.exists(db_path):
         with np.load(db_path) as z:
-            best = dict(zip(z["seeds"].tolist(), z["best"].tolist()))
+            times = dict(zip(z["seeds"].tolist(), z["times_ms"]))
     timer = None
-    mats, classes, xs, B = [], [], [], 0
+    mats, rows, xs, B = [], [], [], 0
     for seed in range(BATCH_SEEDS[0], BATCH_SEEDS[0] + count):
         p = workloads.batch_params(seed)
         rp, ci, v, x = workloads.generate(sb, p)
         m = n = p["rows"]
-        if seed not in best:
+        if seed not in times:
             import torch
 
             timer = timer or tuning.Timer(torch, "cuda")
-            _, best[seed], _ = tuning.exhaustive(sb, timer, rp, ci, v, m, n, tuning.BATCHABLE, reps=5)
+            t, _, _ = tuning.exhaustive(sb, timer, rp, ci, v, m, n, tuning.BATCHABLE, reps=5)
+            times[seed] = np.array([t.get(k, np.nan) for k in range(len(tuning.CLASSES))])
         mats.append((rp, ci, v, m, n))
-        classes.append(int(best[seed]))
+        rows.append(times[seed])
         xs.append(x)
         B += algorithmic_bytes(m, n, int(rp[-1]))
+    # the batch-level choice over the matrices' exhaustive timings (tuning.batch_plan)
+    classes = [int(k) for k in tuning.batch_plan(np.array(rows))]
     return mats, classes, xs, B
 
 

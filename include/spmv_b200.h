@@ -93,7 +93,8 @@ extern "C" {
  *                    kernels (4, 8 and the FP32 default) never hand a stage to the row
  *                    warps, so the row warps' wait runs out: a test of the timeout path
  *                    that faults nothing.                                      default 0
- *   kernel          -1: the format's default (10 for SELL-C-sigma with C = 32 and no
+ *   kernel          -1: the format's default (10 for slices of 32 rows -- SELL-C-sigma
+ *                       with C = 32, sell / sell_sorted with vec_len 32 -- without a
  *                       block_nnz, 8 for other SELL-C-sigma, 2 for DIV-RF with 32
  *                       lanes, 4 for the others);
  *                    0: CTA staged kernel (bulk copy + shared-memory gather, every format);
@@ -120,8 +121,11 @@ extern "C" {
  *                       between lanes (no x buffer);
  *                   10: FP64 slices of exactly 32 rows: warps claim runs of slices from a
  *                       queue (the heaviest slices first) and sum them from registers, the
- *                       next tile's columns and values loaded while this tile is summed,
- *                       x transposed between lanes (no shared memory).
+ *                       next tile's columns and values loaded while this tile is summed and
+ *                       the lines two tiles on prefetched into L1, x transposed between
+ *                       lanes (no shared memory).  Its knobs: stages 1 = no prefetch,
+ *                       4 = prefetch into L2; block_nnz = prefetch distance (entries);
+ *                       block_rows = work-item size in 256-entry tiles.
  *                    DIV-RF: 0 = one CTA per packet (any lane count), 2 = one warp per
  *                    packet, one lane per lane stream (32 lanes).             default -1
  */

@@ -454,8 +454,8 @@ static int build_tiled_cols(Handle & h, const int32_t * d_P, int64_t U, int V)
 	return SPMV_OK;
 }
 
-// Kernel choice: -1 = the format's default (the register-tiled warp kernel for SELL-C-sigma
-// with C = 32, the tiled warp-specialised kernel for wider slices, the warp-specialised
+// Kernel choice: -1 = the format's default (the register-tiled warp kernel for slices of 32
+// rows, the tiled warp-specialised kernel for wider SELL-C-sigma slices, the warp-specialised
 // kernel otherwise: the fastest of each on the 4M-row configuration); 0 = CTA
 // staged kernel; 1 = direct column-major kernel (slices of >= 32 rows only); 2 =
 // warp-autonomous staged kernel (slices of <= 32 rows); 3 = CTA staged kernel with the next
@@ -470,11 +470,17 @@ int build_exec(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
 	int k = h.desc.kernel;
 	if (k < 0) {
-		// measured on the 4M-row matrix: kernel 4 is the fastest for csr_naive (0.196-0.207 ms),
-		// csr_vec (0.344 against kernel 0's 0.391), sell (0.319 / 0.354) and sell_sorted
-		// (0.341 / 0.371); kernel 10 for SELL-C-sigma with C = 32 (0.230 against kernel 8's
-		// 0.255-0.264), kernel 8 for wider slices or a requested staging block
-		k = h.desc.format == SPMV_FMT_SELL_C_S ? (V == 32 && h.desc.block_nnz == 0 ? 10 : 8) : 4;
+		// measured on the 4M-row matrix: kernel 4 is the fastest for csr_naive (0.193 ms),
+		// csr_vec, and sell / sell_sorted with slices of up to 16 rows; kernel 10 for slices of
+		// exactly 32 rows (SELL-C-sigma 0.213 ms against kernel 8's 0.255-0.266, sell 0.197,
+		// sell_sorted 0.217); kernel 8 for SELL-C-sigma with wider slices.  A requested staging
+		// block selects the staged kernels.
+		const bool sliced = h.desc.format == SPMV_FMT_SELL_C_S || h.desc.format == SPMV_FMT_SELL ||
+				h.desc.format == SPMV_FMT_SELL_SORTED;
+		if (sliced && V == 32 && h.desc.block_nnz == 0)
+			k = 10;
+		else
+			k = h.desc.format == SPMV_FMT_SELL_C_S ? 8 : 4;
 		// a requested staging block too large for their two-stage pipeline (about 220 KB of
 		// shared memory per CTA at 12, 16 or 17 bytes an entry) goes to the CTA staged kernel,
 		// which stages fewer blocks at once

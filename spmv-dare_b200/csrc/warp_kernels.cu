@@ -478,31 +478,6 @@ __device__ __forceinline__ double tile_sum(const TileRegArgs & a, const int32_t 
 	return acc;
 }
 
-// PF 3: the full tiles through two fixed register slots, the loop unrolled by two, so the
-// next tile's loads land in the slot the previous iteration consumed (no register moves of
-// data still in flight).
-template <int PF>
-__device__ __forceinline__ double tile_reg_full_tiles(const TileRegArgs & a, int64_t b, int nt, int lane, int R)
-{
-	double acc = 0.0;
-	int32_t c0[8], c1[8];
-	double v0[8], v1[8];
-	if (nt > 0)
-		tile_load(a, b, lane, R, c0, v0);
-	for (int t = 0; t < nt;) {
-		if (t + 1 < nt)
-			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, c1, v1);
-		acc = tile_sum(a, c0, v0, lane, acc);
-		if (++t >= nt)
-			break;
-		if (t + 1 < nt)
-			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, c0, v0);
-		acc = tile_sum(a, c1, v1, lane, acc);
-		++t;
-	}
-	return acc;
-}
-
 template <int PF>
 __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R)
 {
@@ -512,11 +487,9 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 	double acc = 0.0;
 	int32_t c[8], cn[8];
 	double v[8], vn[8];
-	if (PF == 3)
-		acc = tile_reg_full_tiles<PF>(a, b, nt, lane, R);
-	else if (nt > 0)
+	if (nt > 0)
 		tile_load(a, b, lane, R, c, v);
-	for (int t = 0; PF != 3 && t < nt; t++) {
+	for (int t = 0; t < nt; t++) {
 		tile_prefetch<PF>(a, b + (int64_t) t * 256, e_end, lane);
 		if (t + 1 < nt)
 			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, cn, vn);
@@ -817,9 +790,11 @@ int build_warp_chunks(Handle & h, const int32_t * d_P, int64_t U, int V)
 
 // Work items of kernel 10: slices of at least TILE_REG_HEAVY entries alone, the heaviest
 // first; the others in matrix order, in runs of consecutive slices of about
-// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2); block_rows sets the item
-// size in 256-entry tiles instead (the heavy threshold is twice the item size).
-constexpr int64_t TILE_REG_HEAVY = 4096, TILE_REG_ITEM = 2048;
+// TILE_REG_ITEM entries (neighbouring rows keep x warm in L2; the line prefetch runs across
+// the slices of an item); block_rows sets the item size in 256-entry tiles instead (the
+// heavy threshold is twice the item size).  4,096 / 8,192 measured fastest on the 4M-row
+// matrix with the L1 prefetch (0.213 ms; 2,048 / 4,096: 0.217, 8,192 / 16,384: 0.231).
+constexpr int64_t TILE_REG_HEAVY = 8192, TILE_REG_ITEM = 4096;
 
 int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 {
@@ -859,7 +834,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<0>, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<1>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -895,15 +870,14 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		// stages 3 / 4: lines two tiles ahead prefetched into L1 / L2
-		if (h.desc.stages == 3)
-			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		// the lines pf_dist entries ahead prefetched into L1 (default), into L2 (stages 4), or
+		// not at all (stages 1)
+		if (h.desc.stages == 1)
+			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.desc.stages == 5)          // two fixed register slots, loop unrolled by two
-			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
-			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}

@@ -81,6 +81,19 @@ for _i, _c in enumerate(CLASSES):
         BATCHABLE.append(_i)
 
 
+def batch_plan(times, tol=0.05):
+    """Per-matrix classes of a batch from its matrices' exhaustive timings (times[i][k], ms):
+    csr_naive (the default class) for every matrix when the sum of its times is within `tol`
+    of the per-matrix best sum, since an all-csr_naive batch runs as one block-diagonal
+    SpMV on the warp-specialised kernel, about twice the throughput of the mixed-format
+    work queue; otherwise each matrix's own best class."""
+    t = np.where(np.isfinite(times), times, np.inf)
+    best = np.argmin(t, axis=1)
+    if np.sum(t[:, DEFAULT_CLASS]) <= (1.0 + tol) * np.sum(t[np.arange(t.shape[0]), best]):
+        return np.full(t.shape[0], DEFAULT_CLASS)
+    return best
+
+
 def class_name(i):
     c = CLASSES[i]
     rest = ",".join(f"{k}={v}" for k, v in c.items() if k != "format")
