@@ -54,14 +54,13 @@ FALLBACK_HBM = 6650.0
 # that changes the operation order (csr_vec lanes, slice heights) is held to the stated
 # tolerance against csr_naive instead of bit parity.
 TUNED = {
-    "csr_naive": [dict(pack_cols=1), dict(pack_cols=1, block_nnz=1024),
-                  dict(kernel=4, threads=192, block_rows=64, block_nnz=1024, stages=3),
+    "csr_naive": [dict(pack_cols=1), dict(kernel=4, threads=192, block_rows=64, block_nnz=1024, stages=3),
                   dict(kernel=4, threads=160, block_rows=64, block_nnz=512, stages=3)],
     "csr_vec": [dict(vec_len=8), dict(vec_len=2)],
-    "sell": [dict(vec_len=8), dict(vec_len=16), dict(vec_len=32, kernel=10), dict(vec_len=32, kernel=8)],
-    "sell_sorted": [dict(vec_len=8), dict(vec_len=32, kernel=10), dict(vec_len=32, kernel=8)],
-    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, kernel=10), dict(sellcs_c=32, sellcs_sigma=4096, kernel=10),
-                 dict(sellcs_c=32, sellcs_sigma=32, kernel=10), dict(sellcs_c=64, sellcs_sigma=1024, kernel=8)],
+    "sell": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=4)],
+    "sell_sorted": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=4)],
+    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, stages=4), dict(sellcs_c=32, sellcs_sigma=4096),
+                 dict(sellcs_c=32, sellcs_sigma=32), dict(sellcs_c=64, sellcs_sigma=1024)],
     "div_rf": [dict(vec_len=32), dict(vec_len=32, div_packet_vals=4096), dict(vec_len=32, div_packet_vals=65536)],
 }
 TUNED_TOL = 1e-12
