@@ -826,6 +826,12 @@ struct LaneReader {
 	}
 };
 
+// PF: in groups of one coordinate per value, the lines of the code bytes and coordinates
+// DIVW_PF positions ahead are prefetched into L1 (lane 0: the 128 code bytes of 4
+// positions; lanes 1..: the 128 * cb coordinate bytes), inside the group's full rows.
+constexpr int DIVW_PF = 8;
+
+template <bool PF>
 __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 {
 	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
@@ -871,6 +877,14 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 		uint64_t val = 0;                                   // differences restart in every group
 		if (rf == 1) {
 			for (int pos0 = 0; pos0 < n_i; pos0 += 4) {
+				if (PF && pos0 + DIVW_PF + 4 <= dv) {
+					const int64_t k0 = (int64_t) (pos0 + DIVW_PF) * 32;
+					const int cl = (128 * cb + 127) >> 7;      // coordinate lines of 4 positions
+					const uint8_t * pa = lane == 0 ? codes + kstart + k0
+							: lane <= cl ? coords + (cstart + k0) * cb + (int64_t) (lane - 1) * 128 : nullptr;
+					if (pa)
+						asm volatile("prefetch.global.L1 [%0];" ::"l"(pa));
+				}
 				double vv[4], xv[4];
 				int rr[4];
 				#pragma unroll
@@ -1434,7 +1448,10 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.x = d_x;
 	a.y = d_y;
 	if (h.exec_kernel == 2)
-		div_warp_kernel<<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
+		if (h.desc.stages == 3)                  // code bytes and coordinates prefetched into L1
+			div_warp_kernel<true><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
+		else
+			div_warp_kernel<false><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
 	else
 		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());

@@ -462,12 +462,12 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
         gold, absy = orc.csr_gold(rp, ci, v, x)
         ys = {}
-        for kernel in (0, 2):
-            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel)
+        for kernel, st in ((0, 0), (2, 0), (2, 3)):     # stages 3: the warp decoder's L1 prefetch
+            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel, stages=st)
             for _ in range(2):
-                ys[kernel] = mf.spmv(x, np.full(mf.m, 1.0))
-            assert rel_row_error(ys[kernel], gold, absy) <= TOL, (name, pv, kernel)
-        assert rel_row_error(ys[2], ys[0], absy) <= TOL
+                ys[kernel, st] = mf.spmv(x, np.full(mf.m, 1.0))
+            assert rel_row_error(ys[kernel, st], gold, absy) <= TOL, (name, pv, kernel, st)
+        assert rel_row_error(ys[2, 0], ys[0, 0], absy) <= TOL
     with pytest.raises(sb.SpmvError):
         _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
 
