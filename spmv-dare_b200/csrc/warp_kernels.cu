@@ -456,10 +456,22 @@ __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0,
 	if (PF == 0 || lane >= 24 || p + 256 > e_end)
 		return;
 	const void * addr = lane < 16 ? (const void *) (a.vals + p + lane * 16) : (const void *) (a.tcols + p + (lane - 16) * 32);
-	if (PF == 1)
-		asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
-	else
+	if (PF == 2)
 		asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
+	else
+		asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
+}
+
+// PF 3: the first two tiles of a claimed item asked of L1 (lanes 0-15 / 16-31: the values
+// of tile 0 / tile 1, 16 lines each; the columns of both, 16 lines, by a second prefetch of
+// lanes 0-15), for an item claimed one ahead of the one being summed.
+__device__ __forceinline__ void item_head_prefetch(const TileRegArgs & a, int64_t e0, int64_t e_end, int lane)
+{
+	if (e0 + 512 > e_end)
+		return;
+	asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + e0 + lane * 16));
+	if (lane < 16)
+		asm volatile("prefetch.global.L1 [%0];" ::"l"(a.tcols + e0 + lane * 32));
 }
 
 // x of one full tile (lane L's 8 tiled positions), transposed so that lane L holds its row's
@@ -532,17 +544,40 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 {
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
-	for (;;) {
+	if (PF == 3) {
+		// the next item claimed while this one is summed, its head prefetched
 		unsigned int it = 0;
 		if (lane == 0)
 			it = atomicAdd(&a.queue[0], 1u);
 		it = __shfl_sync(0xffffffffu, it, 0);
-		if ((int64_t) it >= a.nitems)
-			break;
-		const int2 r = a.items[it];
-		const int64_t e_end = a.sptr[r.y];
-		for (int64_t sl = r.x; sl < r.y; sl++)
-			tile_reg_slice<PF>(a, sl, e_end, lane, R);
+		while ((int64_t) it < a.nitems) {
+			unsigned int nx = 0;
+			if (lane == 0)
+				nx = atomicAdd(&a.queue[0], 1u);
+			nx = __shfl_sync(0xffffffffu, nx, 0);
+			if ((int64_t) nx < a.nitems) {
+				const int2 q = a.items[nx];
+				item_head_prefetch(a, a.sptr[q.x], a.sptr[q.y], lane);
+			}
+			const int2 r = a.items[it];
+			const int64_t e_end = a.sptr[r.y];
+			for (int64_t sl = r.x; sl < r.y; sl++)
+				tile_reg_slice<PF>(a, sl, e_end, lane, R);
+			it = nx;
+		}
+	} else {
+		for (;;) {
+			unsigned int it = 0;
+			if (lane == 0)
+				it = atomicAdd(&a.queue[0], 1u);
+			it = __shfl_sync(0xffffffffu, it, 0);
+			if ((int64_t) it >= a.nitems)
+				break;
+			const int2 r = a.items[it];
+			const int64_t e_end = a.sptr[r.y];
+			for (int64_t sl = r.x; sl < r.y; sl++)
+				tile_reg_slice<PF>(a, sl, e_end, lane, R);
+		}
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
 	// finish puts the queue back to zero for the next launch
@@ -876,6 +911,8 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 5)           // items claimed one ahead, their heads prefetched
+			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
 			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());

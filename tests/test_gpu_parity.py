@@ -242,13 +242,15 @@ def test_tiled_kernel_long_slices(sb, orc):
                 assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
-@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (4, {}), (0, dict(block_rows=1, block_nnz=256)),
+@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (4, {}), (5, {}), (5, dict(block_rows=2)),
+                                        (0, dict(block_rows=1, block_nnz=256)),
                                         (0, dict(block_rows=64, block_nnz=2048))])
 @pytest.mark.parametrize("fmt,C,sigma", [("sell_c_s", 32, 512), ("sell_c_s", 32, 32), ("sell_c_s", 32, 4096),
                                          ("sell", 32, 0), ("sell_sorted", 32, 0), ("sell_c_s", 64, 512)])
 def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma, stages, kw2):
     """Kernel 10 (warp-claimed slices of 32 rows summed from registers, no shared memory; the
-    lines two tiles ahead prefetched into L1, stages 1: no prefetch, stages 4: into L2;
+    lines two tiles ahead prefetched into L1, stages 1: no prefetch, stages 4: into L2,
+    stages 5: items claimed one ahead with their first two tiles prefetched;
     block_rows / block_nnz: item size and prefetch distance, 256-entry items included):
     the reference's y bits on every golden case and on a skewed matrix whose heavy slices
     (rows up to 3,000 entries) are claimed first; slice heights other than 32 fall back to
