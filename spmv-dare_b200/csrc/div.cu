@@ -621,6 +621,7 @@ struct DivArgs {
 	int L;
 	const double * x;
 	double * y;
+	int pf;                  // warp decoder: prefetch distance in positions
 };
 
 // Exclusive scan over the threads of each lane (thread t: lane t % L, position t / L in its
@@ -706,6 +707,15 @@ __global__ void __launch_bounds__(DEC_THREADS, 3) div_spmv_kernel(DivArgs a)
 		const int per = (n_i + tpl - 1) / tpl;
 		const int p0 = active ? cidx * per : 0;
 		const int p1 = active ? min(n_i, p0 + per) : 0;
+		// the chunk's coordinates, read only in pass 3, asked of L1 now: rf = 1 groups hold
+		// them for positions [p0, p1) of all L lanes in one range, each of its L threads
+		// prefetches every L-th line of it
+		if (a.pf && rf == 1 && p1 > p0) {
+			const uint8_t * c0 = coords + ((int64_t) cstart + (int64_t) p0 * L) * cb;
+			const int64_t len = (int64_t) (p1 - p0) * L * cb;
+			for (int64_t o = (int64_t) lane * 128; o < len; o += (int64_t) L * 128)
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(c0 + o));
+		}
 		// 1) payload bytes of this chunk
 		int nbytes = 0;
 		for (int pos = p0; pos < p1; pos++)
@@ -827,9 +837,9 @@ struct LaneReader {
 };
 
 // PF: in groups of one coordinate per value, the lines of the code bytes and coordinates
-// DIVW_PF positions ahead are prefetched into L1 (lane 0: the 128 code bytes of 4
-// positions; lanes 1..: the 128 * cb coordinate bytes), inside the group's full rows.
-constexpr int DIVW_PF = 8;
+// a.pf positions ahead (a multiple of 4, 8 by default) are prefetched into L1 (lane 0: the
+// 128 code bytes of 4 positions; lanes 1..: the 128 * cb coordinate bytes), inside the
+// group's full rows (0.744 against 0.830 ms on the 4M-row matrix, 4,096-value packets).
 
 template <bool PF>
 __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
@@ -877,8 +887,8 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
 		uint64_t val = 0;                                   // differences restart in every group
 		if (rf == 1) {
 			for (int pos0 = 0; pos0 < n_i; pos0 += 4) {
-				if (PF && pos0 + DIVW_PF + 4 <= dv) {
-					const int64_t k0 = (int64_t) (pos0 + DIVW_PF) * 32;
+				if (PF && pos0 + a.pf + 4 <= dv) {
+					const int64_t k0 = (int64_t) (pos0 + a.pf) * 32;
 					const int cl = (128 * cb + 127) >> 7;      // coordinate lines of 4 positions
 					const uint8_t * pa = lane == 0 ? codes + kstart + k0
 							: lane <= cl ? coords + (cstart + k0) * cb + (int64_t) (lane - 1) * 128 : nullptr;
@@ -1445,13 +1455,17 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.meta = h.d_pkt_meta;
 	a.npackets = h.num_packets;
 	a.L = h.desc.vec_len;
+	// block_nnz: the warp decoder's prefetch distance in positions (rounded up to 4); stages 1:
+	// neither decoder prefetches
+	a.pf = h.desc.stages == 1 ? 0 : h.desc.block_nnz > 0 ? (int) ((h.desc.block_nnz + 3) & ~3) : 8;
 	a.x = d_x;
 	a.y = d_y;
 	if (h.exec_kernel == 2)
-		if (h.desc.stages == 3)                  // code bytes and coordinates prefetched into L1
-			div_warp_kernel<true><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
-		else
+		// code bytes and coordinates prefetched into L1 a.pf positions ahead (stages 1: not)
+		if (h.desc.stages == 1)
 			div_warp_kernel<false><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
+		else
+			div_warp_kernel<true><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
 	else
 		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());

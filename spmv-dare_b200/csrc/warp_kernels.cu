@@ -869,7 +869,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<1>, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<3>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -905,16 +905,17 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		// the lines pf_dist entries ahead prefetched into L1 (default), into L2 (stages 4), or
-		// not at all (stages 1)
+		// default: the lines pf_dist entries ahead prefetched into L1, items claimed one ahead
+		// with their first two tiles prefetched; stages 3: the in-item prefetch only; 4: it
+		// into L2; 1: no prefetch
 		if (h.desc.stages == 1)
 			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 3)
+			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.desc.stages == 5)           // items claimed one ahead, their heads prefetched
-			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
-			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}

@@ -242,15 +242,15 @@ def test_tiled_kernel_long_slices(sb, orc):
                 assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
-@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (4, {}), (5, {}), (5, dict(block_rows=2)),
+@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (3, {}), (4, {}), (0, dict(block_rows=2)),
                                         (0, dict(block_rows=1, block_nnz=256)),
                                         (0, dict(block_rows=64, block_nnz=2048))])
 @pytest.mark.parametrize("fmt,C,sigma", [("sell_c_s", 32, 512), ("sell_c_s", 32, 32), ("sell_c_s", 32, 4096),
                                          ("sell", 32, 0), ("sell_sorted", 32, 0), ("sell_c_s", 64, 512)])
 def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma, stages, kw2):
     """Kernel 10 (warp-claimed slices of 32 rows summed from registers, no shared memory; the
-    lines two tiles ahead prefetched into L1, stages 1: no prefetch, stages 4: into L2,
-    stages 5: items claimed one ahead with their first two tiles prefetched;
+    lines two tiles ahead prefetched into L1 and items claimed one ahead with their first
+    two tiles prefetched, stages 3: the in-item prefetch only, 4: it into L2, 1: none;
     block_rows / block_nnz: item size and prefetch distance, 256-entry items included):
     the reference's y bits on every golden case and on a skewed matrix whose heavy slices
     (rows up to 3,000 entries) are claimed first; slice heights other than 32 fall back to
@@ -452,6 +452,9 @@ def test_div_rf_other_lane_counts(sb, orc, name, L, pv, threads):
     y = mf.spmv(x, np.full(mf.m, 1.0))
     gold, absy = orc.csr_gold(rp, ci, v, x)
     assert rel_row_error(y, gold, absy) <= TOL
+    # without the decoders' L1 prefetch of the coordinates
+    y1 = _mk(sb, g, "div_rf", num_threads=threads, vec_len=L, div_packet_vals=pv, stages=1).spmv(x, np.full(mf.m, 1.0))
+    assert rel_row_error(y1, gold, absy) <= TOL
 
 
 @pytest.mark.parametrize("pv,threads", [(16384, 8), (4096, 8), (1000, 3), (64, 1)])
@@ -465,12 +468,14 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
         gold, absy = orc.csr_gold(rp, ci, v, x)
         ys = {}
-        for kernel, st in ((0, 0), (2, 0), (2, 3)):     # stages 3: the warp decoder's L1 prefetch
-            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel, stages=st)
+        # the warp decoder with its L1 prefetch (default, and 16 positions ahead) and without it
+        for kernel, st, pd in ((0, 0, 0), (2, 0, 0), (2, 1, 0), (2, 0, 16)):
+            mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel, stages=st,
+                     block_nnz=pd)
             for _ in range(2):
-                ys[kernel, st] = mf.spmv(x, np.full(mf.m, 1.0))
-            assert rel_row_error(ys[kernel, st], gold, absy) <= TOL, (name, pv, kernel, st)
-        assert rel_row_error(ys[2, 0], ys[0, 0], absy) <= TOL
+                ys[kernel, st, pd] = mf.spmv(x, np.full(mf.m, 1.0))
+            assert rel_row_error(ys[kernel, st, pd], gold, absy) <= TOL, (name, pv, kernel, st, pd)
+        assert rel_row_error(ys[2, 0, 0], ys[0, 0, 0], absy) <= TOL
     with pytest.raises(sb.SpmvError):
         _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
 
