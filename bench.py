@@ -66,9 +66,8 @@ TUNED = {
 TUNED_TOL = 1e-12
 # FP32 variant settings timed (the first is the library default); every one sums each row
 # as the same sequential Dot2 chain, so y is the same bits
-FP32_SETTINGS = [dict(), dict(pack_cols=1), dict(threads=256, block_rows=96, block_nnz=1536),
-                 dict(threads=320, block_rows=128, block_nnz=2048), dict(threads=224, block_rows=64, block_nnz=1024),
-                 dict(stages=3, block_nnz=1024)]
+FP32_SETTINGS = [dict(), dict(format="sell_c_s", sellcs_c=32, sellcs_sigma=512), dict(pack_cols=1),
+                 dict(threads=256, block_rows=96, block_nnz=1536), dict(threads=224, block_rows=64, block_nnz=1024)]
 
 
 def load_package():
@@ -515,8 +514,10 @@ def fp32_variant(sb, torch, dev, rp, ci, v, x, args, per_format):
     yd = torch.empty(m, dtype=torch.float32, device=dev)
     legs = {}
     for i, params in enumerate(FP32_SETTINGS):
+        kw = dict(params)
+        fmt = kw.pop("format", "csr_naive")      # FP32 values on CSR, or on 32-row SELL-C-sigma slices
         try:
-            mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format="csr_naive", value_type="f32", **params)
+            mf = sb.csr_to_format(rp, ci, v, m, n, nnz, format=fmt, value_type="f32", **kw)
         except sb.SpmvError:
             continue
         _, per = time_device(mf, xd, yd, args.steps, args.warmup, torch)

@@ -102,8 +102,13 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "values must be SPMV_VALUES_F64 or SPMV_VALUES_F32");
 		return SPMV_ERR_ARG;
 	}
-	if (d.values == SPMV_VALUES_F32 && d.format != SPMV_FMT_CSR_NAIVE) {
-		set_error(SPMV_ERR_ARG, "the FP32 variant stores CSR (format csr_naive)");
+	if (d.values == SPMV_VALUES_F32 && d.format != SPMV_FMT_CSR_NAIVE &&
+			!(d.format == SPMV_FMT_SELL_C_S && d.sellcs_c == 32)) {
+		set_error(SPMV_ERR_ARG, "the FP32 variant stores CSR (format csr_naive) or SELL-C-sigma slices of 32 rows");
+		return SPMV_ERR_ARG;
+	}
+	if (d.values == SPMV_VALUES_F32 && d.format == SPMV_FMT_SELL_C_S && d.kernel != -1) {
+		set_error(SPMV_ERR_ARG, "the FP32 variant on 32-row slices has one kernel (kernel -1)");
 		return SPMV_ERR_ARG;
 	}
 	if (d.block_nnz < 0 || d.block_nnz > 16384 || d.stages < 0 || d.stages > 8 || d.block_rows < 0 ||
@@ -286,7 +291,7 @@ static int convert_all(Handle & h)
 	SPMV_TRY(set_x_span(h));
 	h.name = kNames[h.desc.format];
 	if (h.desc.values == SPMV_VALUES_F32)
-		h.name = "Naive_CSR_F32_Dot2_B200";
+		h.name = h.desc.format == SPMV_FMT_SELL_C_S ? "SELL_C_s_F32_Dot2_B200" : "Naive_CSR_F32_Dot2_B200";
 	return SPMV_OK;
 }
 
@@ -607,6 +612,8 @@ int spmv_export(const spmv_handle * H, int32_t id, void * dst, int64_t * count)
 	case SPMV_ARR_ROW_PTR: return export_copy(h.d_rp, h.m + 1, 4, dst, count);
 	case SPMV_ARR_COL_IND: return export_copy(h.d_ci, h.nnz, 4, dst, count);
 	case SPMV_ARR_VALUES:
+		if (h.desc.values == SPMV_VALUES_F32 && fmt == SPMV_FMT_SELL_C_S)   // FP32 slices, column-major
+			return export_copy(h.d_svals_f, h.sellcs_size, 4, dst, count);
 		if (h.desc.values == SPMV_VALUES_F32)
 			return export_copy(h.d_vf, h.nnz, 4, dst, count);
 		return export_copy(h.d_v, h.nnz, 8, dst, count);

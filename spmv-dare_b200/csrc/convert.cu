@@ -706,6 +706,8 @@ int convert_sellcs(Handle & h)
 				h.d_widths, h.d_sptr, h.d_scols, h.d_svals);
 		SPMV_CUDA_TRY(cudaGetLastError());
 	}
+	if (h.desc.values == SPMV_VALUES_F32)
+		return build_sliced_f32(h);      // the FP32 variant over the same slices (fp32.cu)
 	return build_exec(h, h.d_sptr32, ns, C);
 }
 

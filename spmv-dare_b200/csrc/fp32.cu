@@ -763,6 +763,271 @@ __global__ void conv_kernel_f2d(const float * in, double * out, int64_t n)
 		out[i] = (double) in[i];
 }
 
+// ------------------------------------------------------------------ FP32 over 32-row slices
+// The FP32 variant on SELL-C-sigma slices of 32 rows (format sell_c_s, C = 32): FP32 values
+// column-major per slice as the FP64 layout, and the column indices packed per tile of 8
+// slice columns x 32 rows: the tile's smallest column (base) and a fixed bit width, each
+// entry's offset from the base in tiled row-major order (entry (r, k) of a full tile at
+// position r * 8 + k - k8, as the tiled copy of kernels 8-10).  Padding entries pack 0.
+// Warps claim work items as in kernel 10; per full tile lane L decodes its 8 tiled
+// positions q * 32 + L (row 4q + L/8, column L % 8), loads x, and an 8 x 8 transpose
+// between lanes leaves it its row's 8 x values; its row's Dot2 chain then runs over the
+// row's own entries in column order (padding skipped), so y is the CSR row's sequential
+// Dot2 bit for bit.  The next tile's packed words and values are loaded one tile ahead,
+// the lines two tiles ahead prefetched into L1.
+constexpr int F32S_THREADS = 256;
+
+struct F32SArgs {
+	const int2 * items;
+	int64_t nitems;
+	const int32_t * sptr;     // slice pointers (entries)
+	const int32_t * tptr;     // first tile of each slice
+	const int4 * thdr;        // per tile: {first word (low 32 bits), high bits, base, bit width}
+	const uint32_t * words;   // packed offsets
+	int64_t nwords;
+	const float * vals;       // FP32 values, column-major per slice
+	const int32_t * rlen;     // row length of every sliced row (0 past the last row)
+	const int32_t * ymap;     // row_order
+	const float * x;
+	float * y;
+	int64_t m;
+	unsigned int * queue;
+	unsigned int total_warps;
+};
+
+__device__ __forceinline__ void transpose8f(float (&X)[8], int lane)
+{
+	#pragma unroll
+	for (int b = 1; b < 8; b <<= 1) {
+		const bool up = (lane & b) != 0;
+		#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			if (q & b)
+				continue;
+			const float send = up ? X[q] : X[q | b];
+			const float recv = __shfl_xor_sync(0xffffffffu, send, b);
+			if (up)
+				X[q] = recv;
+			else
+				X[q | b] = recv;
+		}
+	}
+}
+
+__device__ __forceinline__ uint32_t f32s_field(const uint32_t * w, int64_t off, uint32_t bit, int bits)
+{
+	const int64_t i = off + (bit >> 5);
+	const uint32_t v = __funnelshift_r(__ldcs(w + i), __ldcs(w + i + 1), bit & 31);
+	return bits >= 32 ? v : (v & ((1u << bits) - 1u));
+}
+
+// columns and values of full tile t0 (tile header hd) for lane L
+__device__ __forceinline__ void f32s_tile_load(const F32SArgs & a, const int4 & hd, int64_t t0, int lane, int R,
+		int32_t (&c)[8], float (&v)[8])
+{
+	const int64_t off = (int64_t) (uint32_t) hd.x | ((int64_t) hd.y << 32);
+	#pragma unroll
+	for (int q = 0; q < 8; q++)
+		c[q] = hd.z + (int32_t) f32s_field(a.words, off, (uint32_t) (q * 32 + lane) * (uint32_t) hd.w, hd.w);
+	#pragma unroll
+	for (int j = 0; j < 8; j++)
+		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
+}
+
+__device__ __forceinline__ void f32s_slice(const F32SArgs & a, int64_t sl, int64_t e_end, int lane, int R)
+{
+	const int64_t b = a.sptr[sl];
+	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
+	const int nt = W >> 3, rem = W & 7;
+	const int64_t tp = a.tptr[sl];
+	const int len = a.rlen[sl * 32 + R];
+	float s = 0.0f, cc = 0.0f;
+	int32_t c[8], cn[8];
+	float v[8], vn[8];
+	int4 hn = nt > 1 ? a.thdr[tp + 1] : make_int4(0, 0, 0, 0);
+	if (nt > 0)
+		f32s_tile_load(a, a.thdr[tp], b, lane, R, c, v);
+	for (int t = 0; t < nt; t++) {
+		const int64_t t0 = b + (int64_t) t * 256;
+		// the values and header two tiles on into L1 (never past the item's entries)
+		if (t0 + 768 <= e_end) {
+			if (lane < 8)
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + t0 + 512 + lane * 32));
+			else if (lane == 8)
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.thdr + tp + t + 2));
+		}
+		int4 hnn = make_int4(0, 0, 0, 0);
+		if (t + 1 < nt) {
+			f32s_tile_load(a, hn, t0 + 256, lane, R, cn, vn);
+			if (t + 2 < nt)
+				hnn = a.thdr[tp + t + 2];
+		}
+		float X[8];
+		#pragma unroll
+		for (int q = 0; q < 8; q++)
+			X[q] = __ldg(a.x + c[q]);
+		transpose8f(X, lane);
+		#pragma unroll
+		for (int j = 0; j < 8; j++)
+			if (t * 8 + j < len)
+				dot2_step(v[j], X[j], s, cc);
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			c[j] = cn[j];
+			v[j] = vn[j];
+		}
+		hn = hnn;
+	}
+	if (rem > 0) {                               // the narrower last tile: rows at R * rem
+		const int64_t t0 = b + (int64_t) nt * 256;
+		const int4 hd = a.thdr[tp + nt];
+		const int64_t off = (int64_t) (uint32_t) hd.x | ((int64_t) hd.y << 32);
+		#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			if (j < rem && nt * 8 + j < len) {
+				const int32_t col = hd.z + (int32_t) f32s_field(a.words, off, (uint32_t) (R * rem + j) * (uint32_t) hd.w, hd.w);
+				dot2_step(__ldcs(a.vals + t0 + j * 32 + R), __ldg(a.x + col), s, cc);
+			}
+		}
+	}
+	const int64_t row = sl * 32 + R;
+	if (row < a.m)
+		a.y[a.ymap[row]] = __fadd_rn(s, cc);
+}
+
+__global__ void __launch_bounds__(F32S_THREADS, 2) f32s_kernel(F32SArgs a)
+{
+	const int lane = threadIdx.x & 31;
+	const int R = 4 * (lane & 7) + (lane >> 3);
+	for (;;) {
+		unsigned int it = 0;
+		if (lane == 0)
+			it = atomicAdd(&a.queue[0], 1u);
+		it = __shfl_sync(0xffffffffu, it, 0);
+		if ((int64_t) it >= a.nitems)
+			break;
+		const int2 r = a.items[it];
+		const int64_t e_end = a.sptr[r.y];
+		for (int64_t sl = r.x; sl < r.y; sl++)
+			f32s_slice(a, sl, e_end, lane, R);
+	}
+	if (lane == 0 && atomicAdd(&a.queue[1], 1u) == a.total_warps - 1) {
+		atomicExch(&a.queue[0], 0u);
+		atomicExch(&a.queue[1], 0u);
+	}
+}
+
+// ---- conversion kernels of the FP32 slices
+
+// row length of every sliced row (rows past m: 0)
+__global__ void f32s_rowlen_kernel(const int32_t * rp, const int32_t * order, int64_t m, int64_t nrows, int32_t * rlen)
+{
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nrows)
+		return;
+	rlen[i] = i < m ? rp[order[i] + 1] - rp[order[i]] : 0;
+}
+
+__global__ void f32s_tilecount_kernel(const int32_t * sptr, int64_t ns, int64_t * cnt)
+{
+	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= ns)
+		return;
+	const int W = (int) (((int64_t) sptr[s + 1] - sptr[s]) >> 5);
+	cnt[s] = (W + 7) >> 3;
+}
+
+// one warp per slice, lane = slice row: each tile's base, bit width and packed words
+__global__ void f32s_tilebits_kernel(const int32_t * sptr, const int64_t * tptr, const int32_t * scols,
+		const int32_t * rlen, int64_t ns, int4 * thdr, int64_t * nwords)
+{
+	const int64_t sl = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (sl >= ns)
+		return;
+	const int64_t b = sptr[sl];
+	const int W = (int) (((int64_t) sptr[sl + 1] - b) >> 5);
+	const int len = rlen[sl * 32 + lane];
+	for (int k8 = 0, t = 0; k8 < W; k8 += 8, t++) {
+		const int tw = W - k8 < 8 ? W - k8 : 8;
+		int lo = INT32_MAX, hi = INT32_MIN;
+		for (int j = 0; j < tw; j++)
+			if (k8 + j < len) {
+				const int32_t col = scols[b + (int64_t) (k8 + j) * 32 + lane];
+				lo = min(lo, col);
+				hi = max(hi, col);
+			}
+		#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+			hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+		}
+		if (lane == 0) {
+			int bits = 0;
+			if (hi > lo) {
+				const uint32_t span = (uint32_t) (hi - lo);
+				bits = 32 - __clz(span);
+			}
+			thdr[tptr[sl] + t] = make_int4(0, 0, hi >= lo ? lo : 0, bits);
+			nwords[tptr[sl] + t] = (int64_t) tw * bits + 1;   // 32 tw fields of `bits` bits, one spare word
+		}
+	}
+}
+
+__global__ void f32s_tileoff_kernel(const int64_t * off, int64_t ntiles, int4 * thdr)
+{
+	const int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= ntiles)
+		return;
+	thdr[t].x = (int) (uint32_t) (off[t] & 0xffffffffLL);
+	thdr[t].y = (int) (off[t] >> 32);
+}
+
+// one warp per slice, lane = slice row: the offsets from the base packed (atomicOr, the
+// words zeroed first)
+__global__ void f32s_pack_kernel(const int32_t * sptr, const int64_t * tptr, const int32_t * scols, const int32_t * rlen,
+		const int4 * thdr, int64_t ns, uint32_t * words)
+{
+	const int64_t sl = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (sl >= ns)
+		return;
+	const int64_t b = sptr[sl];
+	const int W = (int) (((int64_t) sptr[sl + 1] - b) >> 5);
+	const int len = rlen[sl * 32 + lane];
+	for (int k8 = 0, t = 0; k8 < W; k8 += 8, t++) {
+		const int tw = W - k8 < 8 ? W - k8 : 8;
+		const int4 hd = thdr[tptr[sl] + t];
+		const int bits = hd.w;
+		if (bits == 0)
+			continue;
+		const int64_t off = (int64_t) (uint32_t) hd.x | ((int64_t) hd.y << 32);
+		for (int j = 0; j < tw; j++) {
+			const uint32_t val = k8 + j < len ? (uint32_t) (scols[b + (int64_t) (k8 + j) * 32 + lane] - hd.z) : 0u;
+			const uint64_t bit = (uint64_t) (lane * tw + j) * (uint64_t) bits;
+			const int64_t wi = off + (int64_t) (bit >> 5);
+			const int sh = (int) (bit & 31);
+			atomicOr(&words[wi], val << sh);
+			if (sh + bits > 32)
+				atomicOr(&words[wi + 1], (uint32_t) ((uint64_t) val >> (32 - sh)));
+		}
+	}
+}
+
+__global__ void f32s_i64_to_i32_kernel(const int64_t * in, int32_t * out, int64_t n)
+{
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+		out[i] = (int32_t) in[i];
+}
+
+__global__ void f64_to_f32_copy_kernel(const double * in, float * out, int64_t n)
+{
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+		out[i] = __double2float_rn(in[i]);
+}
+
 }  // namespace
 
 const void * ws_f32_kernel_fn(bool packed)
@@ -889,8 +1154,112 @@ int convert_f32(Handle & h)
 	return SPMV_OK;
 }
 
+// FP32 variant on SELL-C-sigma slices of 32 rows: after convert_sellcs has built the FP64
+// slices (row_order, slice pointers, column-major columns and values), the FP32 values,
+// the row lengths, the packed tiles and kernel 10's work items.
+int build_sliced_f32(Handle & h)
+{
+	cudaStream_t s = h.stream;
+	const int64_t ns = h.nslices, total = h.sellcs_size, nrows = ns * 32;
+	h.exec_kernel = 10;
+	SPMV_TRY(h.alloc(&h.d_svals_f, total + 8));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_svals_f, 0, (total + 8) * sizeof(float), s));
+	if (total > 0) {
+		f64_to_f32_copy_kernel<<<(unsigned) ceil_div(total, 256), 256, 0, s>>>(h.d_svals, h.d_svals_f, total);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	SPMV_TRY(h.alloc(&h.d_srlen, nrows > 0 ? nrows : 1));
+	SPMV_TRY(h.alloc(&h.d_stptr, ns + 1));
+	if (ns > 0) {
+		f32s_rowlen_kernel<<<(unsigned) ceil_div(nrows, 256), 256, 0, s>>>(h.d_rp, h.d_order, h.m, nrows, h.d_srlen);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	DevBuf cnt, tptr64;
+	SPMV_TRY(cnt.alloc((ns + 1) * sizeof(int64_t), s));
+	SPMV_TRY(tptr64.alloc((ns + 1) * sizeof(int64_t), s));
+	if (ns > 0) {
+		f32s_tilecount_kernel<<<(unsigned) ceil_div(ns, 256), 256, 0, s>>>(h.d_sptr32, ns, cnt.as<int64_t>());
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	SPMV_TRY(scan_exclusive(cnt.as<int64_t>(), tptr64.as<int64_t>(), ns, s));
+	int64_t ntiles = 0;
+	SPMV_CUDA_TRY(cudaMemcpyAsync(&ntiles, tptr64.as<int64_t>() + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	if (ntiles > INT32_MAX) {
+		set_error(SPMV_ERR_OVERFLOW, "FP32 slices: %lld tiles, beyond the 32-bit range", (long long) ntiles);
+		return SPMV_ERR_OVERFLOW;
+	}
+	f32s_i64_to_i32_kernel<<<(unsigned) ceil_div(ns + 1, 256), 256, 0, s>>>(tptr64.as<int64_t>(), h.d_stptr, ns + 1);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	SPMV_TRY(h.alloc(&h.d_sthdr, ntiles + 2));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_sthdr, 0, (ntiles + 2) * sizeof(int4), s));
+	DevBuf nw, woff;
+	SPMV_TRY(nw.alloc((ntiles + 1) * sizeof(int64_t), s));
+	SPMV_TRY(woff.alloc((ntiles + 1) * sizeof(int64_t), s));
+	if (ns > 0) {
+		f32s_tilebits_kernel<<<(unsigned) ceil_div(nrows, 256), 256, 0, s>>>(h.d_sptr32, tptr64.as<int64_t>(), h.d_scols,
+				h.d_srlen, ns, h.d_sthdr, nw.as<int64_t>());
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	SPMV_TRY(scan_exclusive(nw.as<int64_t>(), woff.as<int64_t>(), ntiles, s));
+	int64_t nwords = 0;
+	SPMV_CUDA_TRY(cudaMemcpyAsync(&nwords, woff.as<int64_t>() + ntiles, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	if (ntiles > 0) {
+		f32s_tileoff_kernel<<<(unsigned) ceil_div(ntiles, 256), 256, 0, s>>>(woff.as<int64_t>(), ntiles, h.d_sthdr);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	h.swords = nwords;
+	SPMV_TRY(h.alloc(&h.d_swords, nwords + 2));
+	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_swords, 0, (nwords + 2) * sizeof(uint32_t), s));
+	if (ns > 0) {
+		f32s_pack_kernel<<<(unsigned) ceil_div(nrows, 256), 256, 0, s>>>(h.d_sptr32, tptr64.as<int64_t>(), h.d_scols,
+				h.d_srlen, h.d_sthdr, ns, h.d_swords);
+		SPMV_CUDA_TRY(cudaGetLastError());
+	}
+	SPMV_TRY(build_tile_reg(h, h.d_sptr32, ns, 32));
+	int per_sm = h.desc.ctas_per_sm;
+	if (per_sm <= 0) {
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f32s_kernel, F32S_THREADS, 0));
+		if (per_sm < 1)
+			per_sm = 1;
+	}
+	h.grid = h.num_sms * per_sm;
+	h.threads = F32S_THREADS;
+	h.kernels_per_run = h.num_items > 0 ? 1 : 0;
+	SPMV_CUDA_TRY(cudaStreamSynchronize(s));
+	return SPMV_OK;
+}
+
+static int launch_sliced_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
+{
+	if (h.num_items == 0)
+		return SPMV_OK;
+	F32SArgs a{};
+	a.items = h.d_items;
+	a.nitems = h.num_items;
+	a.sptr = h.d_sptr32;
+	a.tptr = h.d_stptr;
+	a.thdr = h.d_sthdr;
+	a.words = h.d_swords;
+	a.nwords = h.swords;
+	a.vals = h.d_svals_f;
+	a.rlen = h.d_srlen;
+	a.ymap = h.d_order;
+	a.x = d_x;
+	a.y = d_y;
+	a.m = h.m;
+	a.queue = h.d_queue;
+	a.total_warps = (unsigned int) h.grid * (F32S_THREADS / 32);
+	f32s_kernel<<<h.grid, F32S_THREADS, 0, s>>>(a);
+	SPMV_CUDA_TRY(cudaGetLastError());
+	return SPMV_OK;
+}
+
 int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 {
+	if (h.desc.format == SPMV_FMT_SELL_C_S)
+		return launch_sliced_f32(h, d_x, d_y, s);
 	if (h.exec_kernel == 7) {
 		if (h.num_empty_rows > 0) {
 			zero_rows_f32_kernel<<<(unsigned) ceil_div(h.num_empty_rows, 256), 256, 0, s>>>(h.d_empty_rows,

@@ -138,6 +138,14 @@ struct Handle {
 	int32_t * d_sptr32 = nullptr;   // the same slice pointers, 32-bit, for the staged kernel
 	int32_t * d_scols = nullptr;
 	double * d_svals = nullptr;
+	// FP32 variant over 32-row slices: FP32 values, row lengths, first tile of each slice,
+	// per-tile headers {first word, high bits, base, bit width} and the packed offsets
+	float * d_svals_f = nullptr;
+	int32_t * d_srlen = nullptr;
+	int32_t * d_stptr = nullptr;
+	int4 * d_sthdr = nullptr;
+	uint32_t * d_swords = nullptr;
+	int64_t swords = 0;
 
 	// DIV-RF
 	int64_t div_bytes = 0;
@@ -198,6 +206,7 @@ int convert_sell(Handle & h, bool sorted);
 int convert_sellcs(Handle & h);
 int convert_div(Handle & h);
 int convert_f32(Handle & h);
+int build_sliced_f32(Handle & h);
 const void * ws_f32_kernel_fn(bool packed);   // the FP32 warp-specialised kernel (geometry queries)
 int build_packed_cols(Handle & h);  // packed column streams of the staged blocks (pack.cu)
 int f32ws_stage_bytes(int cap_al);  // its stage size: 8 bytes per staged entry

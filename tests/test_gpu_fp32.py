@@ -48,6 +48,39 @@ def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
     assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
 
 
+@pytest.mark.parametrize("sigma", [512, 32, 4096])
+def test_fp32_slices_match_dot2_oracle(sb, orc, sigma):
+    """The FP32 variant on SELL-C-sigma slices of 32 rows (FP32 values column-major, column
+    offsets packed per 8 x 32 tile with a base and a fixed bit width, padding skipped): y is
+    the CSR rows' sequential Dot2 bit for bit, through FP32 and FP64 buffers, on every golden
+    case, on rows up to 3,000 entries (heavy slices) and on tiles needing 0 to 22 bits."""
+    cases = [load_golden(n) for n in golden_names()]
+    rng = np.random.default_rng(23)
+    m, n = 30000, 4000000
+    lens = rng.integers(0, 40, m)
+    lens[rng.choice(m, 60, replace=False)] = rng.integers(200, 3000, 60)
+    lens[rng.choice(m, 700, replace=False)] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    spans = 2 ** rng.integers(0, 23, m)
+    ci = np.concatenate([np.sort(rng.choice(max(k, min(n, s)), size=k, replace=False)) + rng.integers(0, n - max(k, min(n, s)) + 1)
+                         if k else np.zeros(0, np.int64) for k, s in zip(lens, spans)]).astype(np.int32)
+    cases.append(dict(row_ptr=rp, col_ind=ci, values=rng.uniform(-1, 1, ci.size), x=rng.uniform(-1, 1, n)))
+    for g in cases:
+        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+        mf = sb.csr_to_format(rp, ci, v, rp.size - 1, x.size, int(rp[-1]), format="sell_c_s", sellcs_c=32,
+                              sellcs_sigma=sigma, value_type="f32")
+        assert mf.format_name == "SELL_C_s_F32_Dot2_B200"
+        ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
+        for _ in range(2):                                # the work queue is reset by each launch
+            y32 = mf.spmv(x.astype(np.float32), np.full(mf.m, 1.0, np.float32))
+            assert np.array_equal(y32.view(np.uint32), ref.view(np.uint32)), (rp.size - 1, sigma)
+        y64 = mf.spmv(x, np.full(mf.m, 1.0))
+        assert np.array_equal(y64.astype(np.float32).view(np.uint32), ref.view(np.uint32))
+    with pytest.raises(sb.SpmvError):
+        sb.csr_to_format(rp, ci, v, rp.size - 1, x.size, int(rp[-1]), format="sell_c_s", sellcs_c=64,
+                         sellcs_sigma=512, value_type="f32")
+
+
 @pytest.mark.parametrize("block_nnz", [0, 256, 3072])
 def test_fp32_packed_columns_match_dot2_oracle(sb, orc, block_nnz):
     """pack_cols=1: the kernel reads the column indices packed per staged block (smallest

@@ -70,7 +70,7 @@ def test_div_round_trip(orc, name):
 
 
 def test_restatement_matches_reference_normal100k(orc):
-    """Config 1 at full size against the reference compiled from its sources."""
+    """The 100k-row matrix at full size against the reference compiled from its sources."""
     if not orc.ref_available("div_rf"):
         pytest.skip("reference build (oracle/_ref) not present")
     rp, ci, v, st = orc.ref_generate(100000, 100000, 10, 2, "normal", "random", 0.3, 0, 1.0, 0.5, 14)
