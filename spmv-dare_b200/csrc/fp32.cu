@@ -793,6 +793,7 @@ struct F32SArgs {
 	int64_t m;
 	unsigned int * queue;
 	unsigned int total_warps;
+	int64_t heavy_min;
 };
 
 __device__ __forceinline__ void transpose8f(float (&X)[8], int lane)
@@ -817,7 +818,7 @@ __device__ __forceinline__ void transpose8f(float (&X)[8], int lane)
 __device__ __forceinline__ uint32_t f32s_field(const uint32_t * w, int64_t off, uint32_t bit, int bits)
 {
 	const int64_t i = off + (bit >> 5);
-	const uint32_t v = __funnelshift_r(__ldcs(w + i), __ldcs(w + i + 1), bit & 31);
+	const uint32_t v = __funnelshift_r(__ldg(w + i), __ldg(w + i + 1), bit & 31);   // neighbouring lanes share words
 	return bits >= 32 ? v : (v & ((1u << bits) - 1u));
 }
 
@@ -834,7 +835,7 @@ __device__ __forceinline__ void f32s_tile_load(const F32SArgs & a, const int4 & 
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
-__device__ __forceinline__ void f32s_slice(const F32SArgs & a, int64_t sl, int64_t e_end, int lane, int R)
+__device__ __forceinline__ void f32s_slice(const F32SArgs & a, int64_t sl, int64_t e_end, int lane, int R, int dist)
 {
 	const int64_t b = a.sptr[sl];
 	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
@@ -849,12 +850,20 @@ __device__ __forceinline__ void f32s_slice(const F32SArgs & a, int64_t sl, int64
 		f32s_tile_load(a, a.thdr[tp], b, lane, R, c, v);
 	for (int t = 0; t < nt; t++) {
 		const int64_t t0 = b + (int64_t) t * 256;
-		// the values and header two tiles on into L1 (never past the item's entries)
-		if (t0 + 768 <= e_end) {
-			if (lane < 8)
-				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + t0 + 512 + lane * 32));
-			else if (lane == 8)
-				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.thdr + tp + t + 2));
+		// the values, header and (about) the packed words of the tile dist entries on into L1
+		// (never past the item's entries or the packed words)
+		if (t0 + dist + 256 <= e_end) {
+			const int ahead = dist >> 8;
+			if (lane < 8) {
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + t0 + dist + lane * 32));
+			} else if (lane == 8) {
+				asm volatile("prefetch.global.L1 [%0];" ::"l"(a.thdr + tp + t + ahead));
+			} else if (lane < 14 && hn.w > 0) {
+				const int64_t w = ((int64_t) (uint32_t) hn.x | ((int64_t) hn.y << 32)) + (int64_t) (ahead - 1) * (8 * hn.w + 1) +
+						(int64_t) (lane - 9) * 32;
+				if (w < a.nwords)
+					asm volatile("prefetch.global.L1 [%0];" ::"l"(a.words + w));
+			}
 		}
 		int4 hnn = make_int4(0, 0, 0, 0);
 		if (t + 1 < nt) {
@@ -908,8 +917,10 @@ __global__ void __launch_bounds__(F32S_THREADS, 2) f32s_kernel(F32SArgs a)
 			break;
 		const int2 r = a.items[it];
 		const int64_t e_end = a.sptr[r.y];
+		// a heavy slice (an item of its own) prefetches four times as far ahead
+		const int dist = (r.y - r.x == 1 && e_end - a.sptr[r.x] >= a.heavy_min) ? 2048 : 512;
 		for (int64_t sl = r.x; sl < r.y; sl++)
-			f32s_slice(a, sl, e_end, lane, R);
+			f32s_slice(a, sl, e_end, lane, R, dist);
 	}
 	if (lane == 0 && atomicAdd(&a.queue[1], 1u) == a.total_warps - 1) {
 		atomicExch(&a.queue[0], 0u);
@@ -1251,6 +1262,7 @@ static int launch_sliced_f32(Handle & h, const float * d_x, float * d_y, cudaStr
 	a.m = h.m;
 	a.queue = h.d_queue;
 	a.total_warps = (unsigned int) h.grid * (F32S_THREADS / 32);
+	a.heavy_min = h.tile_heavy_min;
 	f32s_kernel<<<h.grid, F32S_THREADS, 0, s>>>(a);
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;

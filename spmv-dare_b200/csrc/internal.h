@@ -107,6 +107,7 @@ struct Handle {
 	int32_t * d_tcols = nullptr; // kernels 8-10: slice column indices, row-major in 8-column tiles
 	int2 * d_items = nullptr;    // kernel 10: work items (slice ranges), heaviest first
 	int64_t num_items = 0;
+	int64_t tile_heavy_min = 0;  // kernel 10: slices at least this long are items of their own
 	unsigned int * d_queue = nullptr;  // kernel 10: work-queue head and finished-warp count
 	int4 * d_pinfo = nullptr;    // packed columns: per block {16-byte offset, base, bits, bytes}
 	uint32_t * d_pcols = nullptr;  // packed columns: the block streams

@@ -430,6 +430,7 @@ struct TileRegArgs {
 	unsigned int * queue;          // [0] next item, [1] warps done: zero at launch, reset on exit
 	unsigned int total_warps;
 	int pf_dist;                   // line prefetch distance in entries (a multiple of 256)
+	int64_t heavy_min;             // items of one slice this long prefetch 4 x pf_dist ahead
 };
 
 constexpr int TILE_REG_THREADS = 256;
@@ -450,9 +451,9 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 // requested into L1 / L2 by one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the
 // 1 KB of columns), so that tile's register loads find them close.
 template <int PF>
-__device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0, int64_t e_end, int lane)
+__device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0, int64_t e_end, int lane, int dist)
 {
-	const int64_t p = t0 + a.pf_dist;
+	const int64_t p = t0 + dist;
 	if (PF == 0 || lane >= 24 || p + 256 > e_end)
 		return;
 	const void * addr = lane < 16 ? (const void *) (a.vals + p + lane * 16) : (const void *) (a.tcols + p + (lane - 16) * 32);
@@ -491,7 +492,8 @@ __device__ __forceinline__ double tile_sum(const TileRegArgs & a, const int32_t 
 }
 
 template <int PF>
-__device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R)
+__device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R,
+		int dist)
 {
 	const int64_t b = a.sptr[sl];
 	const int W = (int) (((int64_t) a.sptr[sl + 1] - b) >> 5);
@@ -502,7 +504,7 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 	if (nt > 0)
 		tile_load(a, b, lane, R, c, v);
 	for (int t = 0; t < nt; t++) {
-		tile_prefetch<PF>(a, b + (int64_t) t * 256, e_end, lane);
+		tile_prefetch<PF>(a, b + (int64_t) t * 256, e_end, lane, dist);
 		if (t + 1 < nt)
 			tile_load(a, b + (int64_t) (t + 1) * 256, lane, R, cn, vn);
 		double X[8];
@@ -561,8 +563,11 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 			}
 			const int2 r = a.items[it];
 			const int64_t e_end = a.sptr[r.y];
+			// a heavy slice is one warp's long sequential stream: its lines go four times as
+			// far ahead (the SpMV waits on the last such item to finish)
+			const int dist = (r.y - r.x == 1 && e_end - a.sptr[r.x] >= a.heavy_min) ? 4 * a.pf_dist : a.pf_dist;
 			for (int64_t sl = r.x; sl < r.y; sl++)
-				tile_reg_slice<PF>(a, sl, e_end, lane, R);
+				tile_reg_slice<PF>(a, sl, e_end, lane, R, dist);
 			it = nx;
 		}
 	} else {
@@ -575,8 +580,11 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 				break;
 			const int2 r = a.items[it];
 			const int64_t e_end = a.sptr[r.y];
+			// a heavy slice is one warp's long sequential stream: its lines go four times as
+			// far ahead (the SpMV waits on the last such item to finish)
+			const int dist = (r.y - r.x == 1 && e_end - a.sptr[r.x] >= a.heavy_min) ? 4 * a.pf_dist : a.pf_dist;
 			for (int64_t sl = r.x; sl < r.y; sl++)
-				tile_reg_slice<PF>(a, sl, e_end, lane, R);
+				tile_reg_slice<PF>(a, sl, e_end, lane, R, dist);
 		}
 	}
 	// every warp has made its last claim before it counts itself done: the last one to
@@ -844,6 +852,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	std::vector<int2> heavy, rest;
 	const int64_t item = h.desc.block_rows > 0 ? (int64_t) h.desc.block_rows * 256 : TILE_REG_ITEM;
 	const int64_t heavy_min = h.desc.block_rows > 0 ? 2 * item : TILE_REG_HEAVY;
+	h.tile_heavy_min = heavy_min;
 	int64_t u = 0;
 	while (u < U) {
 		const int64_t len = (int64_t) P[u + 1] - P[u];
@@ -896,6 +905,7 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		a.total_warps = (unsigned int) h.grid * (TILE_REG_THREADS / 32);
 		// block_nnz: the line prefetch distance in entries (whole tiles; default two tiles)
 		a.pf_dist = h.desc.block_nnz > 0 ? (int) (ceil_div(h.desc.block_nnz, 256) * 256) : 512;
+		a.heavy_min = h.tile_heavy_min;
 		if (h.desc.format == SPMV_FMT_SELL_C_S) {
 			a.sptr = h.d_sptr32;
 			a.vals = h.d_svals;
