@@ -457,7 +457,7 @@ __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0,
 	if (PF == 0 || lane >= 24 || p + 256 > e_end)
 		return;
 	const void * addr = lane < 16 ? (const void *) (a.vals + p + lane * 16) : (const void *) (a.tcols + p + (lane - 16) * 32);
-	if (PF == 2)
+	if (PF == 2 || PF == 4)
 		asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
 	else
 		asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
@@ -466,13 +466,20 @@ __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0,
 // PF 3: the first two tiles of a claimed item asked of L1 (lanes 0-15 / 16-31: the values
 // of tile 0 / tile 1, 16 lines each; the columns of both, 16 lines, by a second prefetch of
 // lanes 0-15), for an item claimed one ahead of the one being summed.
+template <int PF>
 __device__ __forceinline__ void item_head_prefetch(const TileRegArgs & a, int64_t e0, int64_t e_end, int lane)
 {
 	if (e0 + 512 > e_end)
 		return;
-	asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + e0 + lane * 16));
-	if (lane < 16)
-		asm volatile("prefetch.global.L1 [%0];" ::"l"(a.tcols + e0 + lane * 32));
+	if (PF == 4) {
+		asm volatile("prefetch.global.L2 [%0];" ::"l"(a.vals + e0 + lane * 16));
+		if (lane < 16)
+			asm volatile("prefetch.global.L2 [%0];" ::"l"(a.tcols + e0 + lane * 32));
+	} else {
+		asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vals + e0 + lane * 16));
+		if (lane < 16)
+			asm volatile("prefetch.global.L1 [%0];" ::"l"(a.tcols + e0 + lane * 32));
+	}
 }
 
 // x of one full tile (lane L's 8 tiled positions), transposed so that lane L holds its row's
@@ -546,7 +553,7 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 {
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
-	if (PF == 3) {
+	if (PF == 3 || PF == 4) {
 		// the next item claimed while this one is summed, its head prefetched
 		unsigned int it = 0;
 		if (lane == 0)
@@ -559,7 +566,7 @@ __global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegAr
 			nx = __shfl_sync(0xffffffffu, nx, 0);
 			if ((int64_t) nx < a.nitems) {
 				const int2 q = a.items[nx];
-				item_head_prefetch(a, a.sptr[q.x], a.sptr[q.y], lane);
+				item_head_prefetch<PF>(a, a.sptr[q.x], a.sptr[q.y], lane);
 			}
 			const int2 r = a.items[it];
 			const int64_t e_end = a.sptr[r.y];
@@ -924,6 +931,8 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 4)
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 6)           // the claimed-ahead form with every prefetch into L2
+			tile_reg_kernel<4><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
 			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
