@@ -841,8 +841,9 @@ struct LaneReader {
 // 128 code bytes of 4 positions; lanes 1..: the 128 * cb coordinate bytes), inside the
 // group's full rows (0.744 against 0.830 ms on the 4M-row matrix, 4,096-value packets).
 
-template <bool PF>
-__global__ void __launch_bounds__(DIVW_WARPS * 32) div_warp_kernel(DivArgs a)
+// MINB: CTAs an SM the registers are held to (3: 79 registers; 4: 64, a few spilled)
+template <bool PF, int MINB>
+__global__ void __launch_bounds__(DIVW_WARPS * 32, MINB) div_warp_kernel(DivArgs a)
 {
 	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1460,14 +1461,19 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 	a.pf = h.desc.stages == 1 ? 0 : h.desc.block_nnz > 0 ? (int) ((h.desc.block_nnz + 3) & ~3) : 8;
 	a.x = d_x;
 	a.y = d_y;
-	if (h.exec_kernel == 2)
-		// code bytes and coordinates prefetched into L1 a.pf positions ahead (stages 1: not)
+	if (h.exec_kernel == 2) {
+		// code bytes and coordinates prefetched into L1 a.pf positions ahead (stages 1: not);
+		// ctas_per_sm 4: the form held to 64 registers
+		const unsigned g = (unsigned) ceil_div(h.num_packets, DIVW_WARPS);
 		if (h.desc.stages == 1)
-			div_warp_kernel<false><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
+			div_warp_kernel<false, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+		else if (h.desc.ctas_per_sm == 4)
+			div_warp_kernel<true, 4><<<g, DIVW_WARPS * 32, 0, s>>>(a);
 		else
-			div_warp_kernel<true><<<(unsigned) ceil_div(h.num_packets, DIVW_WARPS), DIVW_WARPS * 32, 0, s>>>(a);
-	else
+			div_warp_kernel<true, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+	} else {
 		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
+	}
 	SPMV_CUDA_TRY(cudaGetLastError());
 	return SPMV_OK;
 }

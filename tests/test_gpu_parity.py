@@ -469,12 +469,13 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         gold, absy = orc.csr_gold(rp, ci, v, x)
         ys = {}
         # the warp decoder with its L1 prefetch (default, and 16 positions ahead) and without it
-        for kernel, st, pd in ((0, 0, 0), (2, 0, 0), (2, 1, 0), (2, 0, 16)):
+        # (and the form held to 64 registers, ctas_per_sm 4)
+        for kernel, st, pd, cps in ((0, 0, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (2, 0, 16, 0), (2, 0, 0, 4)):
             mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel, stages=st,
-                     block_nnz=pd)
+                     block_nnz=pd, ctas_per_sm=cps)
             for _ in range(2):
                 ys[kernel, st, pd] = mf.spmv(x, np.full(mf.m, 1.0))
-            assert rel_row_error(ys[kernel, st, pd], gold, absy) <= TOL, (name, pv, kernel, st, pd)
+            assert rel_row_error(ys[kernel, st, pd], gold, absy) <= TOL, (name, pv, kernel, st, pd, cps)
         assert rel_row_error(ys[2, 0, 0], ys[0, 0, 0], absy) <= TOL
     with pytest.raises(sb.SpmvError):
         _mk(sb, load_golden("hand6"), "div_rf", vec_len=4, kernel=2)
