@@ -66,8 +66,9 @@ TUNED = {
 TUNED_TOL = 1e-12
 # FP32 variant settings timed (the first is the library default); every one sums each row
 # as the same sequential Dot2 chain, so y is the same bits
-FP32_SETTINGS = [dict(), dict(format="sell_c_s", sellcs_c=32, sellcs_sigma=512), dict(pack_cols=1),
-                 dict(threads=256, block_rows=96, block_nnz=1536), dict(threads=224, block_rows=64, block_nnz=1024)]
+FP32_SETTINGS = [dict(), dict(row_assign=1), dict(row_assign=1, threads=256, block_rows=96),
+                 dict(format="sell_c_s", sellcs_c=32, sellcs_sigma=512), dict(pack_cols=1),
+                 dict(threads=256, block_rows=96, block_nnz=1536)]
 
 
 def load_package():

@@ -77,6 +77,10 @@ extern "C" {
  *                        reads a device copy of the column indices packed per staged block
  *                        (smallest column + a fixed bit width), 0 = plain int32 columns.
  *                        Values, y and the exported arrays are unchanged.        default 0
+ *   row_assign           FP32 variant on its warp-specialised kernel: 1 = the row threads of
+ *                        a staged block take its rows longest first, so a row warp's 32
+ *                        rows have similar lengths; 0 = in row order.  y is unchanged.
+ *                                                                                default 0
  *   exact                1: every row is summed in the reference format's own order
  *                        (bit-identical y); 0: rows longer than one staged block are
  *                        reduced in parallel (tolerance parity; kernels 0 and 3 only,
@@ -149,7 +153,8 @@ typedef struct spmv_format_desc {
 	int32_t debug_flags;
 	int32_t div_packet_reordering;
 	int32_t pack_cols;
-	int32_t reserved[2];
+	int32_t row_assign;
+	int32_t reserved;
 } spmv_format_desc;
 
 #define SPMV_DEBUG_WITHHOLD_HANDOFF 1

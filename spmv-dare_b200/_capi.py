@@ -54,7 +54,7 @@ class FormatDesc(ctypes.Structure):
         ("exact", c_int32), ("values", c_int32), ("block_nnz", c_int32), ("block_rows", c_int32),
         ("stages", c_int32), ("ctas_per_sm", c_int32), ("kernel", c_int32), ("threads", c_int32),
         ("wait_limit_us", c_int32), ("debug_flags", c_int32), ("div_packet_reordering", c_int32),
-        ("pack_cols", c_int32), ("reserved", c_int32 * 2),
+        ("pack_cols", c_int32), ("row_assign", c_int32), ("reserved", c_int32),
     ]
 
 

@@ -90,6 +90,14 @@ static int check_desc(const spmv_format_desc & d)
 		set_error(SPMV_ERR_ARG, "pack_cols applies to csr_naive (FP64) and the FP32 variant");
 		return SPMV_ERR_ARG;
 	}
+	if (d.row_assign != 0 && d.row_assign != 1) {
+		set_error(SPMV_ERR_ARG, "row_assign must be 0 or 1 (got %d)", d.row_assign);
+		return SPMV_ERR_ARG;
+	}
+	if (d.row_assign == 1 && (d.values != SPMV_VALUES_F32 || d.format != SPMV_FMT_CSR_NAIVE)) {
+		set_error(SPMV_ERR_ARG, "row_assign applies to the FP32 variant on CSR");
+		return SPMV_ERR_ARG;
+	}
 	if (d.div_packet_reordering != 0 && d.div_packet_reordering != 1) {
 		set_error(SPMV_ERR_ARG, "div_packet_reordering must be 0 or 1 (got %d)", d.div_packet_reordering);
 		return SPMV_ERR_ARG;

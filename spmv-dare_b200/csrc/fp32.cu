@@ -203,6 +203,7 @@ struct F32WsArgs {
 	int hold;                // SPMV_DEBUG_WITHHOLD_HANDOFF: gather warps never hand a stage over
 	const int4 * pinfo;      // packed columns: per block {16-byte offset, base, bits, stream bytes}
 	const uint32_t * pcols;  // packed columns: the streams (pack.cu)
+	const uint16_t * rassign;  // row_assign 1: local row of each row thread, longest rows first
 };
 
 // Column of entry e of a packed block stream (pack.cu): two whole words and a funnel shift.
@@ -373,8 +374,9 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 		const StagedBlock d = sdesc[s];
 		const int64_t e0 = (int64_t) d.elem0 & ~(int64_t) 3;
 		int js = 0, je = 0;
+		int64_t r = -1;                  // this thread's row: by position, or longest first (rassign)
 		if (d.units >= 0 && rt < d.units) {
-			const int64_t r = (int64_t) d.unit0 + rt;
+			r = (int64_t) d.unit0 + (a.rassign ? (int64_t) a.rassign[(int64_t) d.unit0 + rt] : rt);
 			js = (int) ((int64_t) __ldg(a.rp + r) - e0);
 			je = (int) ((int64_t) __ldg(a.rp + r + 1) - e0);
 		}
@@ -396,7 +398,7 @@ __global__ void __launch_bounds__(512) ws_f32_kernel(F32WsArgs a)
 				#pragma unroll 4
 				for (int j = js; j < je; j++)
 					dot2_step(sv[j], xg[j], sum, c);
-				a.y[(int64_t) d.unit0 + rt] = __fadd_rn(sum, c);
+				a.y[r] = __fadd_rn(sum, c);
 			}
 		} else if (rt == 0) {
 			const int flags = -d.units - 1;
@@ -1032,6 +1034,28 @@ __global__ void f32s_i64_to_i32_kernel(const int64_t * in, int32_t * out, int64_
 		out[i] = (int32_t) in[i];
 }
 
+// row_assign 1: per staged block of whole rows, its rows ranked longest first (ties in row
+// order); rassign[unit0 + rank] = local row, so the 32 threads of a row warp take rows of
+// similar length and the warp's Dot2 loops run nearly as long as its threads' rows.  One CTA
+// a block, the block's row lengths in shared memory.
+__global__ void row_rank_kernel(const StagedBlock * blocks, const int32_t * rp, uint16_t * rassign)
+{
+	__shared__ int32_t len[1024];
+	const StagedBlock d = blocks[blockIdx.x];
+	if (d.units <= 0 || d.units > 1024)
+		return;
+	for (int i = threadIdx.x; i < d.units; i += blockDim.x)
+		len[i] = rp[(int64_t) d.unit0 + i + 1] - rp[(int64_t) d.unit0 + i];
+	__syncthreads();
+	for (int i = threadIdx.x; i < d.units; i += blockDim.x) {
+		const int li = len[i];
+		int rank = 0;
+		for (int j = 0; j < d.units; j++)
+			rank += (len[j] > li) || (len[j] == li && j < i);
+		rassign[(int64_t) d.unit0 + rank] = (uint16_t) i;
+	}
+}
+
 __global__ void f64_to_f32_copy_kernel(const double * in, float * out, int64_t n)
 {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -1134,6 +1158,15 @@ int convert_f32(Handle & h)
 			return st;
 		if (h.desc.pack_cols == 1)
 			SPMV_TRY(build_packed_cols(h));
+		if (h.desc.row_assign == 1 && h.num_blocks > 0) {
+			if (h.row_threads > 1024) {
+				set_error(SPMV_ERR_ARG, "row_assign 1 takes at most 1024 row threads (got %d)", h.row_threads);
+				return SPMV_ERR_ARG;
+			}
+			SPMV_TRY(h.alloc(&h.d_rassign, h.m > 0 ? h.m : 1));
+			row_rank_kernel<<<(unsigned) h.num_blocks, 128, 0, s>>>(h.d_blocks, h.d_rp, h.d_rassign);
+			SPMV_CUDA_TRY(cudaGetLastError());
+		}
 		h.kernels_per_run = h.num_blocks > 0 ? 1 : 0;
 		return SPMV_OK;
 	}
@@ -1325,6 +1358,7 @@ int launch_spmv_f32(Handle & h, const float * d_x, float * d_y, cudaStream_t s)
 		w.hold = (h.desc.debug_flags & SPMV_DEBUG_WITHHOLD_HANDOFF) != 0;
 		w.pinfo = h.d_pinfo;
 		w.pcols = h.d_pcols;
+		w.rassign = h.d_rassign;
 		if (h.d_pcols)
 			ws_f32_kernel<true><<<h.grid, h.threads, h.smem_bytes, s>>>(w);
 		else

@@ -109,6 +109,7 @@ struct Handle {
 	int64_t num_items = 0;
 	int64_t tile_heavy_min = 0;  // kernel 10: slices at least this long are items of their own
 	unsigned int * d_queue = nullptr;  // kernel 10: work-queue head and finished-warp count
+	uint16_t * d_rassign = nullptr;  // FP32 kernel 4, row_assign 1: local row of each row thread
 	int4 * d_pinfo = nullptr;    // packed columns: per block {16-byte offset, base, bits, bytes}
 	uint32_t * d_pcols = nullptr;  // packed columns: the block streams
 	int64_t packed_bytes = 0;

@@ -64,6 +64,8 @@ def test_symmetric_unexpanded_is_rejected(sb):
     (dict(format="sell_c_s", kernel=10, value_type="f32"), 1),   # kernel 10 is FP64 slices
     (dict(format="csr_naive", wait_limit_us=-5), 1),
     (dict(format="csr_naive", debug_flags=4), 1),
+    (dict(format="csr_naive", row_assign=2, value_type="f32"), 1),
+    (dict(format="csr_naive", row_assign=1), 1),                 # FP32 variant only
 ])
 def test_invalid_parameters_are_rejected_before_any_device_work(sb, params, status):
     rp = np.array([0, 1], np.int32)

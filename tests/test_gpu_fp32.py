@@ -48,6 +48,19 @@ def test_fp32_variant_matches_dot2_oracle(sb, orc, name, kernel):
     assert rel_row_error(y32.astype(np.float64), gold, absy) <= TOL_F32
 
 
+@pytest.mark.parametrize("kw", [dict(row_assign=1), dict(row_assign=1, block_nnz=256), dict(row_assign=1, threads=512,
+                                                                                          block_rows=256)])
+def test_fp32_longest_first_rows_match_dot2_oracle(sb, orc, kw):
+    """row_assign 1 (the row threads of a block take its rows longest first): the same bits."""
+    for name in golden_names():
+        g = load_golden(name)
+        rp, ci, v, x = g["row_ptr"], g["col_ind"], g["values"], g["x"]
+        mf, y32, y64 = _run(sb, rp, ci, v, x, **kw)
+        ref = orc.csr_f32_dot2(rp, ci, v.astype(np.float32), x.astype(np.float32))
+        assert np.array_equal(y32.view(np.uint32), ref.view(np.uint32)), (name, kw)
+        assert np.array_equal(y64.astype(np.float32).view(np.uint32), y32.view(np.uint32))
+
+
 @pytest.mark.parametrize("sigma", [512, 32, 4096])
 def test_fp32_slices_match_dot2_oracle(sb, orc, sigma):
     """The FP32 variant on SELL-C-sigma slices of 32 rows (FP32 values column-major, column
