@@ -57,18 +57,18 @@ TUNED = {
     "csr_naive": [dict(pack_cols=1), dict(kernel=4, threads=192, block_rows=64, block_nnz=1024, stages=3),
                   dict(kernel=4, threads=160, block_rows=64, block_nnz=512, stages=3)],
     "csr_vec": [dict(vec_len=8), dict(vec_len=2)],
-    "sell": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=4)],
-    "sell_sorted": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=4)],
-    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, stages=4), dict(sellcs_c=32, sellcs_sigma=4096),
+    "sell": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=5)],
+    "sell_sorted": [dict(vec_len=16), dict(vec_len=32), dict(vec_len=32, stages=5)],
+    "sell_c_s": [dict(sellcs_c=32, sellcs_sigma=512, stages=5), dict(sellcs_c=32, sellcs_sigma=4096),
                  dict(sellcs_c=32, sellcs_sigma=32), dict(sellcs_c=64, sellcs_sigma=1024)],
-    "div_rf": [dict(vec_len=32), dict(vec_len=32, div_packet_vals=4096), dict(vec_len=32, div_packet_vals=65536)],
+    "div_rf": [dict(vec_len=32), dict(vec_len=32, div_packet_vals=4096), dict(vec_len=32, div_packet_vals=2048),
+               dict(vec_len=32, div_packet_vals=1024)],
 }
 TUNED_TOL = 1e-12
 # FP32 variant settings timed (the first is the library default); every one sums each row
 # as the same sequential Dot2 chain, so y is the same bits
-FP32_SETTINGS = [dict(), dict(row_assign=1), dict(row_assign=1, threads=256, block_rows=96),
-                 dict(format="sell_c_s", sellcs_c=32, sellcs_sigma=512), dict(pack_cols=1),
-                 dict(threads=256, block_rows=96, block_nnz=1536)]
+FP32_SETTINGS = [dict(), dict(row_assign=1), dict(format="sell_c_s", sellcs_c=32, sellcs_sigma=512),
+                 dict(pack_cols=1), dict(threads=256, block_rows=96, block_nnz=1536)]
 
 
 def load_package():

@@ -126,10 +126,11 @@ extern "C" {
  *                   10: FP64 slices of exactly 32 rows: warps claim runs of slices from a
  *                       queue (the heaviest slices first) and sum them from registers, the
  *                       next tile's columns and values loaded while this tile is summed and
- *                       the lines two tiles on prefetched into L1, x transposed between
+ *                       the lines two tiles on prefetched into L2, x transposed between
  *                       lanes (no shared memory).  Its knobs: stages 1 = no prefetch,
- *                       4 = prefetch into L2; block_nnz = prefetch distance (entries);
- *                       block_rows = work-item size in 256-entry tiles.
+ *                       3 = prefetch into L1, 5 / 6 = into L1 / L2 with items claimed one
+ *                       ahead; block_nnz = prefetch distance (entries); block_rows =
+ *                       work-item size in 256-entry tiles.
  *                    DIV-RF: 0 = one CTA per packet (any lane count), 2 = one warp per
  *                    packet, one lane per lane stream (32 lanes).             default -1
  */

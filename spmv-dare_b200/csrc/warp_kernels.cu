@@ -885,7 +885,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<3>, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<2>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -922,19 +922,20 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			a.vals = h.d_a;
 			a.ymap = h.desc.format == SPMV_FMT_SELL_SORTED ? h.d_rev : nullptr;
 		}
-		// default: the lines pf_dist entries ahead prefetched into L1, items claimed one ahead
-		// with their first two tiles prefetched; stages 3: the in-item prefetch only; 4: it
-		// into L2; 1: no prefetch
+		// default: the lines pf_dist entries ahead (4 x inside a heavy slice) prefetched into L2
+		// (0.2109 ms on the 4M-row SELL-C-sigma matrix); stages 3: into L1 (0.2221); 5: into
+		// L1, items claimed one ahead with their first two tiles prefetched (0.2130); 6: that
+		// form into L2 (0.2130); 1: no prefetch (0.2350)
 		if (h.desc.stages == 1)
 			tile_reg_kernel<0><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 3)
 			tile_reg_kernel<1><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.desc.stages == 4)
-			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.desc.stages == 6)           // the claimed-ahead form with every prefetch into L2
+		else if (h.desc.stages == 5)
+			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+		else if (h.desc.stages == 6)
 			tile_reg_kernel<4><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
-			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
+			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
 		return SPMV_OK;
 	}

@@ -242,15 +242,15 @@ def test_tiled_kernel_long_slices(sb, orc):
                 assert _eq_bits(y, ref).size == 0, (C, kernel, kw)
 
 
-@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (3, {}), (4, {}), (6, {}), (0, dict(block_rows=2)),
+@pytest.mark.parametrize("stages,kw2", [(0, {}), (1, {}), (3, {}), (5, {}), (6, {}), (5, dict(block_rows=2)),
                                         (0, dict(block_rows=1, block_nnz=256)),
                                         (0, dict(block_rows=64, block_nnz=2048))])
 @pytest.mark.parametrize("fmt,C,sigma", [("sell_c_s", 32, 512), ("sell_c_s", 32, 32), ("sell_c_s", 32, 4096),
                                          ("sell", 32, 0), ("sell_sorted", 32, 0), ("sell_c_s", 64, 512)])
 def test_register_tiled_kernel_matches_reference(sb, orc, fmt, C, sigma, stages, kw2):
     """Kernel 10 (warp-claimed slices of 32 rows summed from registers, no shared memory; the
-    lines two tiles ahead prefetched into L1 and items claimed one ahead with their first
-    two tiles prefetched, stages 3: the in-item prefetch only, 4: it into L2, 1: none;
+    lines two tiles ahead prefetched into L2, stages 3: into L1, 5: into L1 with items claimed
+    one ahead and their first two tiles prefetched, 6: that form into L2, 1: none;
     block_rows / block_nnz: item size and prefetch distance, 256-entry items included):
     the reference's y bits on every golden case and on a skewed matrix whose heavy slices
     (rows up to 3,000 entries) are claimed first; slice heights other than 32 fall back to
