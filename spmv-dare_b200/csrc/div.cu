@@ -836,13 +836,14 @@ struct LaneReader {
 	}
 };
 
-// PF: in groups of one coordinate per value, the lines of the code bytes and coordinates
-// a.pf positions ahead (a multiple of 4, 8 by default) are prefetched into L1 (lane 0: the
-// 128 code bytes of 4 positions; lanes 1..: the 128 * cb coordinate bytes), inside the
-// group's full rows (0.744 against 0.830 ms on the 4M-row matrix, 4,096-value packets).
+// PF 1 / 2: in groups of one coordinate per value, the lines of the code bytes and
+// coordinates a.pf positions ahead (a multiple of 4, 8 by default) are prefetched into L1 /
+// L2 (lane 0: the 128 code bytes of 4 positions; lanes 1..: the 128 * cb coordinate bytes),
+// inside the group's full rows (L1: 0.744 against 0.830 ms on the 4M-row matrix, 4,096-value
+// packets).
 
 // MINB: CTAs an SM the registers are held to (3: 79 registers; 4: 64, a few spilled)
-template <bool PF, int MINB>
+template <int PF, int MINB>
 __global__ void __launch_bounds__(DIVW_WARPS * 32, MINB) div_warp_kernel(DivArgs a)
 {
 	__shared__ double ys_all[DIVW_WARPS][DEC_MAX_ROWS];
@@ -893,7 +894,9 @@ __global__ void __launch_bounds__(DIVW_WARPS * 32, MINB) div_warp_kernel(DivArgs
 					const int cl = (128 * cb + 127) >> 7;      // coordinate lines of 4 positions
 					const uint8_t * pa = lane == 0 ? codes + kstart + k0
 							: lane <= cl ? coords + (cstart + k0) * cb + (int64_t) (lane - 1) * 128 : nullptr;
-					if (pa)
+					if (pa && PF == 2)
+						asm volatile("prefetch.global.L2 [%0];" ::"l"(pa));
+					else if (pa)
 						asm volatile("prefetch.global.L1 [%0];" ::"l"(pa));
 				}
 				double vv[4], xv[4];
@@ -1466,11 +1469,13 @@ int launch_div(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 		// ctas_per_sm 4: the form held to 64 registers
 		const unsigned g = (unsigned) ceil_div(h.num_packets, DIVW_WARPS);
 		if (h.desc.stages == 1)
-			div_warp_kernel<false, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+			div_warp_kernel<0, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+		else if (h.desc.stages == 4)            // into L2 instead of L1
+			div_warp_kernel<2, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
 		else if (h.desc.ctas_per_sm == 4)
-			div_warp_kernel<true, 4><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+			div_warp_kernel<1, 4><<<g, DIVW_WARPS * 32, 0, s>>>(a);
 		else
-			div_warp_kernel<true, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
+			div_warp_kernel<1, 3><<<g, DIVW_WARPS * 32, 0, s>>>(a);
 	} else {
 		div_spmv_kernel<<<(unsigned) h.num_packets, DEC_THREADS, 0, s>>>(a);
 	}

@@ -470,7 +470,7 @@ def test_div_rf_warp_decoder(sb, orc, pv, threads):
         ys = {}
         # the warp decoder with its L1 prefetch (default, and 16 positions ahead) and without it
         # (and the form held to 64 registers, ctas_per_sm 4)
-        for kernel, st, pd, cps in ((0, 0, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (2, 0, 16, 0), (2, 0, 0, 4)):
+        for kernel, st, pd, cps in ((0, 0, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (2, 0, 16, 0), (2, 0, 0, 4), (2, 4, 0, 0)):
             mf = _mk(sb, g, "div_rf", num_threads=threads, vec_len=32, div_packet_vals=pv, kernel=kernel, stages=st,
                      block_nnz=pd, ctas_per_sm=cps)
             for _ in range(2):
