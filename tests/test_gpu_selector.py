@@ -108,9 +108,9 @@ def test_training_learns_a_separable_rule(sb):
 
 
 def test_trained_selector_regret_and_gain(sb):
-    """Trained by the library's kernels on the committed autotuning database (3,368 matrices,
-    seeds 0-3367, rows log-uniform in [1e4, 2e6], 29 classes) and judged on 1,759 held-out
-    matrices (seeds 50000-51758) against the exhaustive autotuner:
+    """Trained by the library's kernels on the committed autotuning database (6,074 matrices,
+    seeds 0-6073, rows log-uniform in [1e4, 2e6], 29 classes) and judged on 2,000 held-out
+    matrices (seeds 50000-51999) against the exhaustive autotuner:
     * within 5% of exhaustive-autotune throughput on average;
     * better than the method without it (the library default class) on average;
     * at >= 100x lower tuning cost (device features + one forward pass against the
