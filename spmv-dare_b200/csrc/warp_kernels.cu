@@ -548,8 +548,8 @@ __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl
 		a.y[a.ymap ? (int64_t) a.ymap[row] : row] = acc;
 }
 
-template <int PF, int MINB = 2>
-__global__ void __launch_bounds__(TILE_REG_THREADS, MINB) tile_reg_kernel(TileRegArgs a)
+template <int PF>
+__global__ void __launch_bounds__(TILE_REG_THREADS, 2) tile_reg_kernel(TileRegArgs a)
 {
 	const int lane = threadIdx.x & 31;
 	const int R = 4 * (lane & 7) + (lane >> 3);
@@ -885,8 +885,7 @@ int build_tile_reg(Handle & h, const int32_t * d_P, int64_t U, int V)
 	SPMV_CUDA_TRY(cudaMemsetAsync(h.d_queue, 0, 2 * sizeof(unsigned int), s));
 	int per_sm = h.desc.ctas_per_sm;
 	if (per_sm <= 0) {
-		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-				h.desc.stages == 7 ? tile_reg_kernel<2, 3> : tile_reg_kernel<2>, TILE_REG_THREADS, 0));
+		SPMV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_reg_kernel<2>, TILE_REG_THREADS, 0));
 		if (per_sm < 1)
 			per_sm = 1;
 	}
@@ -935,8 +934,6 @@ int launch_warp(Handle & h, const double * d_x, double * d_y, cudaStream_t s)
 			tile_reg_kernel<3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else if (h.desc.stages == 6)
 			tile_reg_kernel<4><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
-		else if (h.desc.stages == 7)           // the default form held to 3 CTAs an SM (80 registers, spills)
-			tile_reg_kernel<2, 3><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		else
 			tile_reg_kernel<2><<<h.grid, TILE_REG_THREADS, 0, s>>>(a);
 		SPMV_CUDA_TRY(cudaGetLastError());
