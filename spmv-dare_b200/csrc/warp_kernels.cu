@@ -446,10 +446,12 @@ __device__ __forceinline__ void tile_load(const TileRegArgs & a, int64_t t0, int
 		v[j] = __ldcs(a.vals + t0 + j * 32 + R);
 }
 
-// PF 1 / 2: the cache lines of the tile pf_dist entries ahead (two tiles by default; across
-// slice boundaries: an item's slices are contiguous; never past the item's end e_end)
-// requested into L1 / L2 by one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the
-// 1 KB of columns), so that tile's register loads find them close.
+// The prefetch forms of kernel 10 (template PF): 0 none; 1 / 2 the cache lines of the tile
+// `dist` entries ahead (two tiles by default, eight in a heavy slice; across slice boundaries:
+// an item's slices are contiguous; never past the item's end e_end) requested into L1 / L2 by
+// one prefetch per lane (lanes 0-15 the 2 KB of values, 16-23 the 1 KB of columns), so that
+// tile's register loads find them close; 3 / 4 the same into L1 / L2 with every item claimed
+// one ahead and its first two tiles prefetched.  2 is the default.
 template <int PF>
 __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0, int64_t e_end, int lane, int dist)
 {
@@ -463,9 +465,9 @@ __device__ __forceinline__ void tile_prefetch(const TileRegArgs & a, int64_t t0,
 		asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
 }
 
-// PF 3: the first two tiles of a claimed item asked of L1 (lanes 0-15 / 16-31: the values
-// of tile 0 / tile 1, 16 lines each; the columns of both, 16 lines, by a second prefetch of
-// lanes 0-15), for an item claimed one ahead of the one being summed.
+// PF 3 / 4: the first two tiles of a claimed item asked of L1 / L2 (lanes 0-31: the 4 KB of
+// values, 32 lines; lanes 0-15: the 2 KB of columns), for an item claimed one ahead of the one
+// being summed.
 template <int PF>
 __device__ __forceinline__ void item_head_prefetch(const TileRegArgs & a, int64_t e0, int64_t e_end, int lane)
 {
