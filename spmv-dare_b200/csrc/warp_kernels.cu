@@ -484,22 +484,6 @@ __device__ __forceinline__ void item_head_prefetch(const TileRegArgs & a, int64_
 	}
 }
 
-// x of one full tile (lane L's 8 tiled positions), transposed so that lane L holds its row's
-// 8 values, and the row's FMA chain continued over them in column order.
-__device__ __forceinline__ double tile_sum(const TileRegArgs & a, const int32_t (&c)[8], const double (&v)[8], int lane,
-		double acc)
-{
-	double X[8];
-	#pragma unroll
-	for (int q = 0; q < 8; q++)
-		X[q] = __ldg(a.x + c[q]);
-	transpose8(X, lane);
-	#pragma unroll
-	for (int j = 0; j < 8; j++)
-		acc = __fma_rn(v[j], X[j], acc);
-	return acc;
-}
-
 template <int PF>
 __device__ __forceinline__ void tile_reg_slice(const TileRegArgs & a, int64_t sl, int64_t e_end, int lane, int R,
 		int dist)
