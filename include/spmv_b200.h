@@ -448,6 +448,12 @@ int64_t spmv_gen_host_check(int64_t rows, int64_t cols, double avg_nnz_per_row, 
 /* Library version string. */
 const char * spmv_version(void);
 
+/* sizeof(spmv_format_desc) and sizeof(spmv_info) as built into the library.  A caller
+ * compiled against another revision of this header compares them with its own sizeof and
+ * stops, instead of the library reading or writing past the caller's structs. */
+size_t spmv_format_desc_size(void);
+size_t spmv_info_size(void);
+
 #ifdef __cplusplus
 }
 #endif

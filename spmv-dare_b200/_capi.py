@@ -104,6 +104,8 @@ SIGNATURES = {
     "spmv_artgen_get": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "spmv_artgen_destroy": (None, [c_void_p]),
     "spmv_version": (c_char_p, []),
+    "spmv_format_desc_size": (ctypes.c_size_t, []),
+    "spmv_info_size": (ctypes.c_size_t, []),
     "spmv_batch_create": (c_void_p, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                      POINTER(c_int)]),
     "spmv_batch_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -146,5 +148,11 @@ def load():
             f = getattr(lib, name)
             f.restype = res
             f.argtypes = args
+        # the structs declared here must be the library's: a stale build would otherwise read
+        # or write past them
+        for name, st in (("spmv_format_desc_size", FormatDesc), ("spmv_info_size", Info)):
+            if getattr(lib, name)() != ctypes.sizeof(st):
+                raise RuntimeError(f"{LIB_PATH}: {name}() = {getattr(lib, name)()} but the binding's struct has "
+                                   f"{ctypes.sizeof(st)} bytes: rebuild the library")
         _lib = lib
     return _lib

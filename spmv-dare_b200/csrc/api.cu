@@ -772,4 +772,14 @@ const char * spmv_version(void)
 	return "spmv_b200 1.0 (sm_100a)";
 }
 
+size_t spmv_format_desc_size(void)
+{
+	return sizeof(spmv_format_desc);
+}
+
+size_t spmv_info_size(void)
+{
+	return sizeof(spmv_info);
+}
+
 }  // extern "C"

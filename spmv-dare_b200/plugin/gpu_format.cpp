@@ -94,6 +94,11 @@ struct GPU_Format : Matrix_Format
 struct Matrix_Format *
 csr_to_format(INT_T * row_ptr, INT_T * col_ind, ValueTypeReference * values, long m, long n, long nnz, long symmetric, long symmetry_expanded)
 {
+	// this translation unit's structs must be the library's (a stale build of either side
+	// would read or write past them)
+	if (spmv_format_desc_size() != sizeof(spmv_format_desc) || spmv_info_size() != sizeof(spmv_info))
+		error("spmv_b200: header and library differ (spmv_format_desc %zu / %zu bytes, spmv_info %zu / %zu): rebuild",
+				sizeof(spmv_format_desc), spmv_format_desc_size(), sizeof(spmv_info), spmv_info_size());
 	spmv_format_desc d;
 	spmv_format_desc_init(&d, GPU_FORMAT_ID);
 	d.num_threads = omp_get_max_threads();

@@ -85,3 +85,40 @@ def test_no_device_reports_status_not_fallback(sb):
 
 def test_statistics_labels(sb):
     assert sb.statistics_print_labels().startswith(",gpu_format")
+
+
+def test_struct_sizes_match_the_binding(sb):
+    """The library's spmv_format_desc / spmv_info are the binding's (checked at load too)."""
+    import ctypes
+
+    from spmv_dare_b200 import _capi
+
+    L = sb.library()
+    assert L.spmv_format_desc_size() == ctypes.sizeof(_capi.FormatDesc)
+    assert L.spmv_info_size() == ctypes.sizeof(_capi.Info)
+
+
+def test_dropin_executable_is_built_against_this_header(tmp_path):
+    """The drop-in driver checks its structs against the library before any GPU work: without
+    a GPU it stops at the device, not at a header mismatch."""
+    import os
+    import subprocess
+
+    from conftest import ROOT
+
+    exe = os.path.join(ROOT, "spmv-dare_b200", "plugin", "_build", "dropin_check_csr_naive_d.exe")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in executables not built (make -C spmv-dare_b200/plugin REF=...)")
+    if has_gpu():
+        pytest.skip("a GPU is present (the GPU tests run the driver)")
+    with open(tmp_path / "a.bin", "wb") as f:
+        np.array([2, 2, 2], np.int64).tofile(f)
+        np.array([0, 1, 2], np.int32).tofile(f)
+        np.array([0, 1], np.int32).tofile(f)
+        np.array([1.0, 2.0]).tofile(f)
+    np.array([1.0, 1.0]).tofile(tmp_path / "x.bin")
+    p = subprocess.run([exe, str(tmp_path / "a.bin"), str(tmp_path / "x.bin"), str(tmp_path / "y.bin")],
+                       capture_output=True, text=True, timeout=120)
+    out = p.stdout + p.stderr
+    assert p.returncode != 0 and "header and library differ" not in out
+    assert "spmv_b200:" in out and "device" in out.lower(), out[-500:]
