@@ -615,7 +615,8 @@ def run_reference(args):
         "config": make_config(args, name, m, n, nnz, B, world),
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
-                         "sample": f"the full 4M-row matrix, {args.steps} timed SpMV steps after {args.warmup} warm-up"},
+                         "sample": f"the {'full 4M-row' if not args.rows else f'{m}-row'} matrix, {args.steps} timed "
+                                   f"SpMV steps after {args.warmup} warm-up"},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

@@ -1,0 +1,33 @@
+"""bench.py --impl reference (the reference's own csr_naive, compiled from its sources, on the
+host cores) prints one JSON line of the bench contract; run here on a 20k-row instance of
+the 4M-row matrix's generator parameters."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+
+def test_reference_arm_prints_the_contract_line():
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_csr_naive.so")):
+        pytest.skip("reference build (oracle/_ref) not present")
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--rows", "20000", "--steps", "3",
+                        "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-1500:]
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["unit"] == "GB/s" and d["value"] > 0 and d["steps"] == 3
+    assert d["n_gpus"] == 1 and d["higher_is_better"] is True and d["dtype"] == "f64"
+    assert d["config"]["m"] == 20000 and d["config"]["format"] == "csr_naive"
+    assert set(d["config"]) == {"workload", "format", "m", "n", "nnz", "bytes_per_spmv", "l2", "parallelism",
+                                "format_params"}
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert "20000-row" in d["cpu_baseline"]["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
