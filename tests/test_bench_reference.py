@@ -31,3 +31,12 @@ def test_reference_arm_prints_the_contract_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
     assert "20000-row" in d["cpu_baseline"]["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun with N > 1 only rank 0 runs and prints; the others exit 0 at once."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--rows", "20000", "--steps", "3",
+                        "--warmup", "3", "--gpus", "2"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-1500:]
+    assert not [l for l in p.stdout.splitlines() if l.startswith("{")]
