@@ -40,3 +40,18 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--warmup", "3", "--gpus", "2"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stderr[-1500:]
     assert not [l for l in p.stdout.splitlines() if l.startswith("{")]
+
+
+def test_bench_bytes_and_workload_names():
+    """Algorithmic bytes of one SpMV on the 4M-row matrix (csr_mem_footprint + x + y) and of
+    the FP32 variant; workload names carry no configuration numbering."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert bench.algorithmic_bytes(4000000, 4000000, 80469735) == 1045636824
+    assert bench.algorithmic_bytes(100000, 100000, 999475) == 13993704
+    assert 80469735 * 8 + 4000001 * 4 + 4000000 * 4 + 4000000 * 4 == 691757884
+    assert "4Mx4M" in bench.WORKLOAD and "config" not in bench.WORKLOAD.lower()
+    assert bench.batch_workload(128).startswith("batch: 128 artificial matrices, seeds 1000-1127")
